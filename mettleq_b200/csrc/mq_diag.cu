@@ -1,0 +1,269 @@
+// Diagonal phase layers (b): RZ / U1 / Z / S / T, CZ / CPHASE / CRZ, ZZ and
+// any mix of them, in ONE streaming pass.
+//
+// Replaces diag_pair_layer / diag_weighted_layer (shaders/diag.py:19-217),
+// zz_chain_layer / zz_weighted_layer (shaders/zz.py:16-185) and the per-gate
+// apply_diagonal passes of the CPU path (sim.py:94-138, device.py:1154-1211).
+//
+// The reference multiplies one unit phase per equal-angle group inside the
+// kernel (zz.py:40-71); here the host factors the whole diagonal into at most
+// eight lookup tables, each indexed by a window of <= 10 index bits (or by a
+// short list of scattered bits for far-apart pairs).  Every term's phase is
+// folded into exactly one table in double precision, so a 29-bond chain with
+// all-different angles costs four table reads and four complex products per
+// amplitude, independent of the number of bonds.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <vector>
+
+#include "mq_internal.cuh"
+
+namespace mq {
+
+struct DiagLut {
+  uint16_t off;
+  uint8_t nbits;
+  uint8_t contig;
+  uint8_t shift;
+  uint8_t pos[11];
+};
+
+constexpr int kMaxLuts = 8;
+template <typename R> struct DiagCap;
+template <> struct DiagCap<float> { static constexpr int v = 2048; };
+template <> struct DiagCap<double> { static constexpr int v = 1024; };
+
+template <typename R>
+struct DiagParams {
+  uint32_t n_pairs;  // 2^(n-1) element pairs
+  int32_t n_luts;
+  uint32_t n_entries;
+  uint32_t pad;
+  DiagLut lut[kMaxLuts];
+  V2<R> e[DiagCap<R>::v];
+};
+
+__device__ __forceinline__ uint32_t lut_index(const DiagLut& L, uint32_t i) {
+  if (L.contig) return (i >> L.shift) & ((1u << L.nbits) - 1u);
+  uint32_t x = 0;
+  for (int k = 0; k < L.nbits; ++k) x |= ((i >> L.pos[k]) & 1u) << k;
+  return x;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_diag(V2<R>* __restrict__ st, const __grid_constant__ DiagParams<R> P) {
+  using T = V2<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* lut = reinterpret_cast<T*>(smem_raw);
+  for (uint32_t j = threadIdx.x; j < P.n_entries; j += blockDim.x) lut[j] = P.e[j];
+  __syncthreads();
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P.n_pairs; p += stride) {
+    const uint32_t i0 = p << 1, i1 = i0 | 1u;
+    T a0 = st[i0], a1 = st[i1];
+    T f0 = mk<R>(1, 0), f1 = mk<R>(1, 0);
+    for (int l = 0; l < P.n_luts; ++l) {
+      const DiagLut& L = P.lut[l];
+      f0 = cmul(f0, lut[L.off + lut_index(L, i0)]);
+      f1 = cmul(f1, lut[L.off + lut_index(L, i1)]);
+    }
+    st[i0] = cmul(a0, f0);
+    st[i1] = cmul(a1, f1);
+  }
+}
+
+// ---------------------------------------------------------------- planner
+struct Term {
+  std::vector<int> bits;                   // global index bits, first = MSB of table index
+  std::vector<std::complex<double>> tab;   // 2^|bits| values
+};
+
+struct PlannedLut {
+  std::vector<int> pos;  // index bit k of the table <- global bit pos[k]
+  bool contig = false;
+  std::vector<std::complex<double>> vals;
+};
+
+static std::complex<double> cis(double t) { return {std::cos(t), std::sin(t)}; }
+
+static int build_terms(int n, int n_terms, const int32_t* kinds, const int32_t* wires, const double* params,
+                       std::vector<Term>& terms, std::complex<double>& scalar) {
+  scalar = 1.0;
+  for (int t = 0; t < n_terms; ++t) {
+    const int kind = kinds[t];
+    const int a = wires[2 * t], b = wires[2 * t + 1];
+    const double* p = params + 8 * t;
+    const bool two = (kind == MQ_DIAG_ZZ || kind == MQ_DIAG_CPHASE || kind == MQ_DIAG_CRZ || kind == MQ_DIAG_2Q);
+    const bool one = (kind == MQ_DIAG_RZ || kind == MQ_DIAG_PHASE || kind == MQ_DIAG_1Q);
+    if (kind == MQ_DIAG_GLOBAL) { scalar *= cis(p[0]); continue; }
+    if (!one && !two) return fail(MQ_EINVAL, "unknown diagonal term kind " + std::to_string(kind));
+    if (a < 0 || a >= n) return fail(MQ_EINVAL, "diagonal term wire out of range");
+    if (two && (b < 0 || b >= n || b == a)) return fail(MQ_EINVAL, "invalid bond (" + std::to_string(a) + ", " + std::to_string(b) + ")");
+    Term tm;
+    const double th = p[0];
+    switch (kind) {
+      case MQ_DIAG_ZZ: tm.tab = {cis(-th), cis(th), cis(th), cis(-th)}; break;
+      case MQ_DIAG_CPHASE: tm.tab = {1.0, 1.0, 1.0, cis(th)}; break;
+      case MQ_DIAG_CRZ: tm.tab = {1.0, 1.0, cis(-th / 2), cis(th / 2)}; break;
+      case MQ_DIAG_2Q:
+        tm.tab = {{p[0], p[1]}, {p[2], p[3]}, {p[4], p[5]}, {p[6], p[7]}};
+        break;
+      case MQ_DIAG_RZ: tm.tab = {cis(-th / 2), cis(th / 2)}; break;
+      case MQ_DIAG_PHASE: tm.tab = {1.0, cis(th)}; break;
+      case MQ_DIAG_1Q: tm.tab = {{p[0], p[1]}, {p[2], p[3]}}; break;
+    }
+    // CZ is CPHASE(pi): use exact -1 (diag.py:89-98 keeps +-1 exact too)
+    if (kind == MQ_DIAG_CPHASE && std::fabs(th - M_PI) < 1e-15) tm.tab[3] = -1.0;
+    if (kind == MQ_DIAG_PHASE && std::fabs(th - M_PI) < 1e-15) tm.tab[1] = -1.0;
+    tm.bits.push_back(n - 1 - a);
+    if (two) tm.bits.push_back(n - 1 - b);
+    terms.push_back(std::move(tm));
+  }
+  return MQ_OK;
+}
+
+static std::complex<double> term_value(const Term& tm, const std::vector<int>& pos, uint32_t x) {
+  uint32_t idx = 0;
+  const int k = (int)tm.bits.size();
+  for (int j = 0; j < k; ++j) {
+    const int gb = tm.bits[j];
+    int lp = (int)(std::find(pos.begin(), pos.end(), gb) - pos.begin());
+    const uint32_t bit = (x >> lp) & 1u;
+    idx |= bit << (k - 1 - j);
+  }
+  return tm.tab[idx];
+}
+
+static void finalize_lut(PlannedLut& L, const std::vector<const Term*>& members) {
+  const uint32_t sz = 1u << L.pos.size();
+  L.vals.assign(sz, 1.0);
+  for (uint32_t x = 0; x < sz; ++x) {
+    std::complex<double> v = 1.0;
+    for (const Term* tm : members) v *= term_value(*tm, L.pos, x);
+    L.vals[x] = v;
+  }
+}
+
+// Greedy factorisation with windows of width <= W.
+static std::vector<PlannedLut> plan_luts(const std::vector<Term>& terms, int W) {
+  std::vector<PlannedLut> luts;
+  std::vector<int> local, far;
+  for (size_t t = 0; t < terms.size(); ++t) {
+    auto [mn, mx] = std::minmax_element(terms[t].bits.begin(), terms[t].bits.end());
+    ((*mx - *mn) < W ? local : far).push_back((int)t);
+  }
+  std::vector<bool> done(terms.size(), false);
+  while (true) {
+    int s = 1 << 30;
+    for (int t : local)
+      if (!done[t]) s = std::min(s, *std::min_element(terms[t].bits.begin(), terms[t].bits.end()));
+    if (s == (1 << 30)) break;
+    std::vector<const Term*> members;
+    int hi = s;
+    for (int t : local) {
+      if (done[t]) continue;
+      auto [mn, mx] = std::minmax_element(terms[t].bits.begin(), terms[t].bits.end());
+      if (*mn >= s && *mx < s + W) { done[t] = true; members.push_back(&terms[t]); hi = std::max(hi, *mx); }
+    }
+    PlannedLut L;
+    for (int b = s; b <= hi; ++b) L.pos.push_back(b);
+    L.contig = true;
+    finalize_lut(L, members);
+    luts.push_back(std::move(L));
+  }
+  // far pairs: scattered-bit tables
+  size_t i = 0;
+  while (i < far.size()) {
+    PlannedLut L;
+    std::vector<const Term*> members;
+    while (i < far.size()) {
+      std::vector<int> pos = L.pos;
+      for (int b : terms[far[i]].bits)
+        if (std::find(pos.begin(), pos.end(), b) == pos.end()) pos.push_back(b);
+      if ((int)pos.size() > W && !members.empty()) break;
+      L.pos = pos;
+      members.push_back(&terms[far[i]]);
+      ++i;
+    }
+    std::sort(L.pos.begin(), L.pos.end());
+    L.contig = true;
+    for (size_t k = 1; k < L.pos.size(); ++k)
+      if (L.pos[k] != L.pos[0] + (int)k) L.contig = false;
+    finalize_lut(L, members);
+    luts.push_back(std::move(L));
+  }
+  return luts;
+}
+
+template <typename R>
+static int launch_diag_pass(mq_state* h, const std::vector<PlannedLut>& luts) {
+  using T = V2<R>;
+  auto* P = new DiagParams<R>();
+  std::memset(P, 0, sizeof(DiagParams<R>));
+  P->n_pairs = (uint32_t)(h->dim() >> 1);
+  P->n_luts = (int32_t)luts.size();
+  uint32_t off = 0;
+  for (size_t l = 0; l < luts.size(); ++l) {
+    const PlannedLut& L = luts[l];
+    DiagLut& d = P->lut[l];
+    d.off = (uint16_t)off;
+    d.nbits = (uint8_t)L.pos.size();
+    d.contig = L.contig ? 1 : 0;
+    d.shift = (uint8_t)(L.pos.empty() ? 0 : L.pos[0]);
+    for (size_t k = 0; k < L.pos.size(); ++k) d.pos[k] = (uint8_t)L.pos[k];
+    for (auto v : L.vals) P->e[off++] = mk<R>((R)v.real(), (R)v.imag());
+  }
+  P->n_entries = off;
+  const size_t smem = sizeof(T) * std::max<uint32_t>(off, 1);
+  const uint32_t pairs = P->n_pairs;
+  const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((pairs + 255) / 256, (uint64_t)h->num_sms * 8));
+  k_diag<R><<<grid, 256, smem, h->stream>>>(reinterpret_cast<T*>(h->cur_buf()), *P);
+  delete P;
+  MQ_LAUNCHED("k_diag");
+  h->launches += 1;
+  h->sweeps += 1;
+  return MQ_OK;
+}
+
+int launch_diag_terms(mq_state* h, int n_terms, const int32_t* kinds, const int32_t* wires, const double* params) {
+  std::vector<Term> terms;
+  std::complex<double> scalar;
+  int rc = build_terms(h->n, n_terms, kinds, wires, params, terms, scalar);
+  if (rc) return rc;
+  if (terms.empty() && scalar == std::complex<double>(1.0, 0.0)) return MQ_OK;
+  const int cap = h->dtype == MQ_C64 ? DiagCap<float>::v : DiagCap<double>::v;
+  std::vector<PlannedLut> luts;
+  for (int W = 10; W >= 1; --W) {
+    luts = plan_luts(terms, W);
+    size_t entries = 0;
+    for (auto& L : luts) entries += L.vals.size();
+    if ((int)luts.size() <= kMaxLuts && (int)entries <= cap) break;
+    if (W == 1) break;  // fall through to multi-pass below
+  }
+  if (luts.empty()) {
+    PlannedLut L;
+    L.contig = true;
+    L.vals = {1.0};
+    luts.push_back(L);
+  }
+  for (auto& v : luts[0].vals) v *= scalar;
+  // Split into passes that respect the parameter-block capacity.
+  size_t i = 0;
+  while (i < luts.size()) {
+    std::vector<PlannedLut> pass;
+    size_t entries = 0;
+    while (i < luts.size() && (int)pass.size() < kMaxLuts && (int)(entries + luts[i].vals.size()) <= cap) {
+      entries += luts[i].vals.size();
+      pass.push_back(luts[i]);
+      ++i;
+    }
+    if (pass.empty()) return fail(MQ_EUNSUPPORTED, "diagonal table exceeds capacity");
+    rc = (h->dtype == MQ_C64) ? launch_diag_pass<float>(h, pass) : launch_diag_pass<double>(h, pass);
+    if (rc) return rc;
+  }
+  return MQ_OK;
+}
+
+}  // namespace mq

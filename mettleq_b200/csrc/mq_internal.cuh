@@ -1,0 +1,116 @@
+// Internal definitions shared by the libmq CUDA sources (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/mq.h"
+
+namespace mq {
+
+// ---------------------------------------------------------------- complex
+template <typename R> struct V2T;
+template <> struct V2T<float> { using T = float2; };
+template <> struct V2T<double> { using T = double2; };
+template <typename R> using V2 = typename V2T<R>::T;
+
+template <typename R> __host__ __device__ __forceinline__ V2<R> mk(R re, R im) {
+  V2<R> v; v.x = re; v.y = im; return v;
+}
+template <typename T> __device__ __forceinline__ T cadd(T a, T b) { a.x += b.x; a.y += b.y; return a; }
+template <typename T> __device__ __forceinline__ T csub(T a, T b) { a.x -= b.x; a.y -= b.y; return a; }
+template <typename T> __device__ __forceinline__ T cmul(T a, T b) {
+  T r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+template <typename T> __device__ __forceinline__ T cmulc(T a, T b) {  // a * conj(b)
+  T r; r.x = a.x * b.x + a.y * b.y; r.y = a.y * b.x - a.x * b.y; return r;
+}
+template <typename T, typename R> __device__ __forceinline__ T cscale(T a, R s) { a.x *= s; a.y *= s; return a; }
+
+// ---------------------------------------------------------------- limits
+constexpr int kMaxQubits = 32;        // 32-bit amplitude indices
+constexpr int kTileMaxC64 = 13;       // 2^13 complex64 = 64 KiB tile
+constexpr int kTileMaxC128 = 12;      // 2^12 complex128 = 64 KiB tile
+
+// ---------------------------------------------------------------- errors
+void set_error(int code, const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* where);
+
+#define MQ_CUDA(call)                                                   \
+  do {                                                                  \
+    cudaError_t _e = (call);                                            \
+    if (_e != cudaSuccess) return ::mq::cuda_fail(_e, #call);           \
+  } while (0)
+
+#define MQ_LAUNCHED(where)                                              \
+  do {                                                                  \
+    cudaError_t _e = cudaGetLastError();                                \
+    if (_e != cudaSuccess) return ::mq::cuda_fail(_e, where);           \
+  } while (0)
+
+}  // namespace mq
+
+// ---------------------------------------------------------------- handle
+struct mq_state {
+  int n = 0;
+  int dtype = MQ_C64;
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  void* buf[2] = {nullptr, nullptr};
+  int cur = 0;
+  size_t state_bytes = 0;
+  void* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  uint64_t launches = 0;
+  uint64_t sweeps = 0;
+
+  size_t amp_bytes() const { return dtype == MQ_C64 ? 8 : 16; }
+  uint64_t dim() const { return uint64_t(1) << n; }
+  void* cur_buf() const { return buf[cur]; }
+};
+
+namespace mq {
+
+// Make the handle's device current for the duration of a call.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int now = -1;
+    if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+  }
+};
+
+int ensure_scratch(mq_state* h, size_t bytes);
+int ensure_alt(mq_state* h);  // allocate the second buffer if absent
+
+// ------------------------------------------------------------ launchers
+// Tile sweeps: U(2) layer and QFT (mq_tile.cu)
+int launch_u2_layer(mq_state* h, const double* mats, const uint8_t* active);
+int launch_qft_contiguous(mq_state* h, int q0, int k, int inverse);
+int launch_qft_stages(mq_state* h, int q0, int k, int j_begin, int j_end, int inverse);
+int launch_cu2_list(mq_state* h, int n_gates, const int32_t* targets, const uint32_t* cmasks, const double* mats);
+// Diagonal layers (mq_diag.cu)
+int launch_diag_terms(mq_state* h, int n_terms, const int32_t* kinds, const int32_t* wires,
+                      const double* params);
+// GF(2) affine permutation, out-of-place into the alternate buffer (mq_perm.cu).
+// cols[j] = A e_j (index-bit columns of the source map), c = flip constant.
+int launch_affine_cols(mq_state* h, const uint32_t* cols, uint32_t c);
+// Reductions (mq_reduce.cu)
+int run_probabilities(mq_state* h, const int32_t* wires, int k, int out_dtype, void* out);
+int run_sample(mq_state* h, const int32_t* wires, int k, uint64_t seed, uint64_t offset,
+               int64_t shots, int64_t* out);
+int run_expval_pauli(mq_state* h, int n_words, const uint64_t* xmask, const uint64_t* zmask,
+                     const int32_t* ny, double* out);
+
+// GF(2) helpers (host)
+bool gf2_invert(int n, const uint32_t* cols, uint32_t* inv_cols);
+
+}  // namespace mq

@@ -1,0 +1,284 @@
+"""Kernel-level statevector API over libmq (the layer calls of the hot path).
+
+``StateVector`` owns one device state (a C-ABI ``mq_state`` handle).  Its
+methods are the B200 counterparts of the reference's Metal layer API
+(shaders/__init__.py:26-56: u2_list_layer_all, diag_weighted_layer,
+zz_weighted_layer, qft_stage_all / qft_stage_sub, xor_affine_gather) and of
+``StateVectorSimulator.probabilities_array`` / ``sample_array``
+(sim.py:322-419).  Every call goes to CUDA; nothing here computes on the host
+beyond argument packing.
+
+Conventions: qubit q is index bit n-1-q (MSB-first, sim.py:10-14).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import Dict, Iterable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _native as N
+
+_DTYPES = {"complex64": N.MQ_C64, "complex128": N.MQ_C128, np.complex64: N.MQ_C64, np.complex128: N.MQ_C128}
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _mats_array(n: int, mats) -> np.ndarray:
+    m = np.asarray(mats, dtype=np.complex128).reshape(n, 4)
+    out = np.empty((n, 8), dtype=np.float64)
+    out[:, 0::2] = m.real
+    out[:, 1::2] = m.imag
+    return np.ascontiguousarray(out)
+
+
+def pauli_masks(n: int, word: Dict[int, str]) -> Tuple[int, int, int]:
+    """(xmask, zmask, ny) over index bits for a Pauli word {wire: 'X'|'Y'|'Z'|'I'}."""
+    x = z = ny = 0
+    for w, p in word.items():
+        w = int(w)
+        p = str(p).upper()
+        if not (0 <= w < n):
+            raise ValueError("Observable wire is outside the device")
+        bit = 1 << (n - 1 - w)
+        if p == "I":
+            continue
+        if p == "X":
+            x |= bit
+        elif p == "Z":
+            z |= bit
+        elif p == "Y":
+            x |= bit
+            z |= bit
+            ny += 1
+        else:
+            raise ValueError("Pauli products support only I, X, Y, and Z")
+    return x, z, ny
+
+
+class StateVector:
+    """One statevector resident in device memory (one CUDA stream)."""
+
+    def __init__(self, n: int, dtype="complex64", device: int = 0, stream: Optional[int] = None):
+        self.n = int(n)
+        if self.n <= 0:
+            raise ValueError("n_qubits must be positive")
+        self.dtype = np.dtype(dtype)
+        if self.dtype not in (np.complex64, np.complex128):
+            raise ValueError("dtype must be complex64 or complex128")
+        self._dt = N.MQ_C64 if self.dtype == np.complex64 else N.MQ_C128
+        self.device = int(device)
+        lib = N.lib()
+        h = C.c_void_p()
+        N.check(lib.mq_state_create(self.n, self._dt, self.device, C.c_void_p(stream or 0), C.byref(h)))
+        self._h = h
+        self._lib = lib
+
+    # -- lifetime -------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.mq_state_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # -- state ----------------------------------------------------------
+    def reset(self) -> None:
+        N.check(self._lib.mq_state_reset(self._h))
+
+    def set(self, vec) -> None:
+        v = np.ascontiguousarray(np.asarray(vec, dtype=self.dtype).reshape(-1))
+        if v.size != (1 << self.n):
+            raise ValueError("state has the wrong length")
+        N.check(self._lib.mq_state_set(self._h, _ptr(v)))
+
+    def get(self) -> np.ndarray:
+        out = np.empty(1 << self.n, dtype=self.dtype)
+        N.check(self._lib.mq_state_get(self._h, _ptr(out)))
+        return out
+
+    def copy_from(self, other: "StateVector") -> None:
+        N.check(self._lib.mq_state_copy(self._h, other._h))
+
+    def set_stream(self, stream: Optional[int]) -> None:
+        N.check(self._lib.mq_state_set_stream(self._h, C.c_void_p(stream or 0)))
+
+    def device_ptr(self) -> int:
+        p = C.c_void_p()
+        N.check(self._lib.mq_state_device_ptr(self._h, C.byref(p)))
+        return int(p.value or 0)
+
+    def synchronize(self) -> None:
+        N.check(self._lib.mq_sync(self._h))
+
+    def counters(self) -> Tuple[int, int]:
+        a, b = C.c_uint64(), C.c_uint64()
+        N.check(self._lib.mq_state_counters(self._h, C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)
+
+    # -- (a) single-qubit layers -------------------------------------
+    def apply_u2_layer(self, mats, active: Optional[Iterable[int]] = None) -> None:
+        """Per-qubit 2x2 unitaries (u2_list_layer_all, single_qubit.py:512-615).
+        ``mats`` is (n, 4) [u00, u01, u10, u11]; ``active`` lists the qubits
+        whose matrices are applied (None = all)."""
+        m = _mats_array(self.n, mats)
+        act = None
+        if active is not None:
+            act = np.zeros(self.n, dtype=np.uint8)
+            for q in active:
+                if not (0 <= int(q) < self.n):
+                    raise ValueError("Qubit index out of range")
+                act[int(q)] = 1
+        N.check(self._lib.mq_apply_u2_layer(self._h, _ptr(m), _ptr(act) if act is not None else None))
+
+    def apply_u2_uniform(self, u2x2) -> None:
+        """The same 2x2 on every qubit (u2_layer_all, single_qubit.py:422-509)."""
+        m = _mats_array(1, u2x2).reshape(8)
+        N.check(self._lib.mq_apply_u2_uniform(self._h, _ptr(m)))
+
+    def apply_single(self, u, q: int) -> None:
+        mats = np.tile(np.eye(2, dtype=np.complex128).reshape(1, 4), (self.n, 1))
+        mats[int(q)] = np.asarray(u, dtype=np.complex128).reshape(4)
+        self.apply_u2_layer(mats, [int(q)])
+
+    def apply_controlled(self, gates: Sequence[Tuple[Sequence[int], int, np.ndarray]]) -> None:
+        """Controlled 2x2 gates in order: (controls, target, matrix)."""
+        if not gates:
+            return
+        targets = np.array([int(t) for _, t, _ in gates], dtype=np.int32)
+        coff = np.zeros(len(gates) + 1, dtype=np.int32)
+        ctl: List[int] = []
+        for i, (cs, _, _) in enumerate(gates):
+            ctl.extend(int(c) for c in cs)
+            coff[i + 1] = len(ctl)
+        controls = np.array(ctl if ctl else [0], dtype=np.int32)
+        mats = _mats_array(len(gates), [np.asarray(u).reshape(4) for _, _, u in gates])
+        N.check(self._lib.mq_apply_controlled_u2(self._h, len(gates), _ptr(targets), _ptr(coff), _ptr(controls),
+                                                 _ptr(mats)))
+
+    # -- (b) diagonal layers -------------------------------------------
+    def apply_diag_terms(self, terms: Sequence[Tuple[int, int, int, Sequence[float]]]) -> None:
+        """Terms (kind, wire_a, wire_b, params) with kinds MQ_DIAG_*; all
+        commute and are applied in one pass."""
+        k = len(terms)
+        if k == 0:
+            return
+        kinds = np.empty(k, dtype=np.int32)
+        wires = np.empty(2 * k, dtype=np.int32)
+        params = np.zeros((k, 8), dtype=np.float64)
+        for i, (kind, a, b, p) in enumerate(terms):
+            kinds[i] = int(kind)
+            wires[2 * i] = int(a)
+            wires[2 * i + 1] = int(b)
+            pp = list(p)
+            params[i, :len(pp)] = pp
+        N.check(self._lib.mq_apply_diag_terms(self._h, k, _ptr(kinds), _ptr(wires), _ptr(params)))
+
+    def apply_zz_weighted(self, bonds: Sequence[Tuple[int, int]], thetas: Sequence[float]) -> None:
+        """exp(-i sum_b theta_b Z_a Z_b) (zz_weighted_layer, zz.py:99-140)."""
+        self._diag_layer(N.MQ_DIAG_ZZ, bonds, thetas)
+
+    def apply_cphase_weighted(self, bonds: Sequence[Tuple[int, int]], thetas: Sequence[float]) -> None:
+        """CPHASE(theta_b) per bond, CZ = pi (diag_weighted_layer, diag.py:123-167)."""
+        self._diag_layer(N.MQ_DIAG_CPHASE, bonds, thetas)
+
+    def _diag_layer(self, kind: int, bonds, thetas) -> None:
+        bonds = list(bonds)
+        thetas = list(thetas)
+        if len(bonds) != len(thetas):
+            raise ValueError("bonds/thetas length mismatch")
+        if not bonds:
+            return
+        b = np.ascontiguousarray(np.asarray(bonds, dtype=np.int32).reshape(-1))
+        t = np.ascontiguousarray(np.asarray(thetas, dtype=np.float64))
+        N.check(self._lib.mq_apply_diag_layer(self._h, int(kind), len(bonds), _ptr(b), _ptr(t)))
+
+    # -- (c) QFT ------------------------------------------------------------
+    def apply_qft(self, wires: Optional[Sequence[int]] = None, inverse: bool = False) -> None:
+        """Ordered-wire QFT without final swaps (sim.py:522-563)."""
+        w = np.ascontiguousarray(np.asarray(list(range(self.n)) if wires is None else list(wires), dtype=np.int32))
+        N.check(self._lib.mq_apply_qft(self._h, _ptr(w), int(w.size), 1 if inverse else 0))
+
+    def apply_qft_stages(self, q0: int, k: int, j_begin: int, j_end: int, inverse: bool = False) -> None:
+        N.check(self._lib.mq_apply_qft_stages(self._h, int(q0), int(k), int(j_begin), int(j_end), 1 if inverse else 0))
+
+    # -- (d) GF(2) affine permutation ------------------------------------
+    def apply_xor_affine(self, rows: Sequence[int], c: int) -> None:
+        """out[y] = in[f^{-1}(y)] with inverse rows/c (xor_affine.py:79-116)."""
+        r = np.ascontiguousarray(np.asarray([int(x) for x in rows], dtype=np.uint64))
+        if r.size != self.n:
+            raise ValueError("rows must have one mask per qubit")
+        N.check(self._lib.mq_apply_xor_affine(self._h, _ptr(r), int(c)))
+
+    # -- (e) probabilities, sampling, expectations ------------------------
+    def probabilities(self, wires: Optional[Sequence[int]] = None, dtype=np.float64) -> np.ndarray:
+        """Full (wires=None) or marginal probabilities, first wire = MSB."""
+        dt = np.dtype(dtype)
+        if dt not in (np.float32, np.float64):
+            raise ValueError("probabilities dtype must be float32 or float64")
+        code = 0 if dt == np.float32 else 1
+        if wires is None:
+            out = np.empty(1 << self.n, dtype=dt)
+            N.check(self._lib.mq_probabilities(self._h, None, -1, code, _ptr(out)))
+            return out
+        w = np.ascontiguousarray(np.asarray(list(wires), dtype=np.int32))
+        out = np.empty(1 << w.size, dtype=dt)
+        N.check(self._lib.mq_probabilities(self._h, _ptr(w) if w.size else _ptr(np.zeros(1, np.int32)),
+                                           int(w.size), code, _ptr(out)))
+        return out
+
+    def sample_indices(self, shots: int, wires: Optional[Sequence[int]] = None, *, seed: int = 0,
+                       stream_offset: int = 0) -> np.ndarray:
+        shots = int(shots)
+        if shots < 0:
+            raise ValueError("shots must be non-negative")
+        out = np.empty(max(shots, 1), dtype=np.int64)
+        if wires is None:
+            N.check(self._lib.mq_sample(self._h, None, -1, int(seed) & 0xFFFFFFFFFFFFFFFF, int(stream_offset),
+                                        shots, _ptr(out)))
+        else:
+            w = np.ascontiguousarray(np.asarray(list(wires), dtype=np.int32))
+            N.check(self._lib.mq_sample(self._h, _ptr(w) if w.size else _ptr(np.zeros(1, np.int32)), int(w.size),
+                                        int(seed) & 0xFFFFFFFFFFFFFFFF, int(stream_offset), shots, _ptr(out)))
+        return out[:shots]
+
+    def sample_bits(self, shots: int, wires: Optional[Sequence[int]] = None, *, seed: int = 0,
+                    stream_offset: int = 0) -> np.ndarray:
+        """Shot bits (shots, k), first requested wire = MSB (sim.py:414-419)."""
+        k = self.n if wires is None else len(list(wires))
+        idx = self.sample_indices(shots, wires, seed=seed, stream_offset=stream_offset)
+        shifts = np.arange(k - 1, -1, -1, dtype=np.int64)
+        return ((idx[:, None] >> shifts) & 1).astype(np.int64)
+
+    def expval_pauli(self, words: Sequence[Dict[int, str]]) -> np.ndarray:
+        """<psi|P|psi> per Pauli word (pauli_product_expectations,
+        integrations/_common.py:384-427), complex128 array."""
+        k = len(words)
+        if k == 0:
+            return np.zeros(0, dtype=np.complex128)
+        xs = np.empty(k, dtype=np.uint64)
+        zs = np.empty(k, dtype=np.uint64)
+        ny = np.empty(k, dtype=np.int32)
+        for i, wd in enumerate(words):
+            x, z, y = pauli_masks(self.n, wd)
+            xs[i], zs[i], ny[i] = x, z, y
+        out = np.empty(2 * k, dtype=np.float64)
+        N.check(self._lib.mq_expval_pauli(self._h, k, _ptr(xs), _ptr(zs), _ptr(ny), _ptr(out)))
+        return out[0::2] + 1j * out[1::2]

@@ -1,0 +1,1 @@
+"""numpy-backed mlx stand-in used only to generate golden vectors."""
