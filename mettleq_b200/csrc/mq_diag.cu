@@ -40,7 +40,7 @@ struct DiagParams {
   uint32_t n_pairs;  // 2^(n-1) element pairs
   int32_t n_luts;
   uint32_t n_entries;
-  uint32_t pad;
+  int32_t n_low;     // tables [0, n_low) read index bits 0-2
   DiagLut lut[kMaxLuts];
   V2<R> e[DiagCap<R>::v];
 };
@@ -52,6 +52,10 @@ __device__ __forceinline__ uint32_t lut_index(const DiagLut& L, uint32_t i) {
   return x;
 }
 
+// Each thread handles aligned groups of 8 consecutive amplitudes (index bits
+// 0-2 vary inside a group).  Tables [0, n_low) read index bits 0-2 and are
+// looked up per amplitude; the product of the remaining tables is the same
+// for the whole group and is computed once.
 template <typename R>
 __global__ void __launch_bounds__(256) k_diag(V2<R>* __restrict__ st, const __grid_constant__ DiagParams<R> P) {
   using T = V2<R>;
@@ -59,18 +63,48 @@ __global__ void __launch_bounds__(256) k_diag(V2<R>* __restrict__ st, const __gr
   T* lut = reinterpret_cast<T*>(smem_raw);
   for (uint32_t j = threadIdx.x; j < P.n_entries; j += blockDim.x) lut[j] = P.e[j];
   __syncthreads();
+  const uint32_t n_groups = P.n_pairs >> 2;  // groups of 8 (n >= 3)
   const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < P.n_pairs; p += stride) {
-    const uint32_t i0 = p << 1, i1 = i0 | 1u;
-    T a0 = st[i0], a1 = st[i1];
-    T f0 = mk<R>(1, 0), f1 = mk<R>(1, 0);
-    for (int l = 0; l < P.n_luts; ++l) {
-      const DiagLut& L = P.lut[l];
-      f0 = cmul(f0, lut[L.off + lut_index(L, i0)]);
-      f1 = cmul(f1, lut[L.off + lut_index(L, i1)]);
+  const int n_low = P.n_low;
+  for (uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x; gi < n_groups; gi += stride) {
+    const uint32_t i0 = gi << 3;
+    T a[8];
+    if constexpr (sizeof(R) == 4) {
+      const float4* p4 = reinterpret_cast<const float4*>(st + i0);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const float4 x = p4[v];
+        a[2 * v] = make_float2(x.x, x.y);
+        a[2 * v + 1] = make_float2(x.z, x.w);
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) a[v] = st[i0 + v];
     }
-    st[i0] = cmul(a0, f0);
-    st[i1] = cmul(a1, f1);
+    T hi = mk<R>(1, 0);
+    for (int l = n_low; l < P.n_luts; ++l) hi = cmul(hi, lut[P.lut[l].off + lut_index(P.lut[l], i0)]);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      T f = hi;
+      for (int l = 0; l < n_low; ++l) f = cmul(f, lut[P.lut[l].off + lut_index(P.lut[l], i0 + v)]);
+      a[v] = cmul(a[v], f);
+    }
+    if constexpr (sizeof(R) == 4) {
+      float4* p4 = reinterpret_cast<float4*>(st + i0);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) p4[v] = make_float4(a[2 * v].x, a[2 * v].y, a[2 * v + 1].x, a[2 * v + 1].y);
+    } else {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) st[i0 + v] = a[v];
+    }
+  }
+  // states of fewer than 8 amplitudes
+  if (n_groups == 0 && blockIdx.x == 0) {
+    for (uint32_t i = threadIdx.x; i < 2 * P.n_pairs; i += blockDim.x) {
+      T f = mk<R>(1, 0);
+      for (int l = 0; l < P.n_luts; ++l) f = cmul(f, lut[P.lut[l].off + lut_index(P.lut[l], i)]);
+      st[i] = cmul(st[i], f);
+    }
   }
 }
 
@@ -198,12 +232,19 @@ static std::vector<PlannedLut> plan_luts(const std::vector<Term>& terms, int W) 
 }
 
 template <typename R>
-static int launch_diag_pass(mq_state* h, const std::vector<PlannedLut>& luts) {
+static int launch_diag_pass(mq_state* h, const std::vector<PlannedLut>& in_luts) {
   using T = V2<R>;
+  std::vector<PlannedLut> luts;
+  for (const auto& L : in_luts)
+    if (!L.pos.empty() && *std::min_element(L.pos.begin(), L.pos.end()) < 3) luts.push_back(L);
+  const int n_low = (int)luts.size();
+  for (const auto& L : in_luts)
+    if (L.pos.empty() || *std::min_element(L.pos.begin(), L.pos.end()) >= 3) luts.push_back(L);
   auto* P = new DiagParams<R>();
   std::memset(P, 0, sizeof(DiagParams<R>));
   P->n_pairs = (uint32_t)(h->dim() >> 1);
   P->n_luts = (int32_t)luts.size();
+  P->n_low = n_low;
   uint32_t off = 0;
   for (size_t l = 0; l < luts.size(); ++l) {
     const PlannedLut& L = luts[l];
@@ -217,8 +258,8 @@ static int launch_diag_pass(mq_state* h, const std::vector<PlannedLut>& luts) {
   }
   P->n_entries = off;
   const size_t smem = sizeof(T) * std::max<uint32_t>(off, 1);
-  const uint32_t pairs = P->n_pairs;
-  const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((pairs + 255) / 256, (uint64_t)h->num_sms * 8));
+  const uint32_t groups = std::max<uint32_t>(1, P->n_pairs >> 2);
+  const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((groups + 255) / 256, (uint64_t)h->num_sms * 8));
   k_diag<R><<<grid, 256, smem, h->stream>>>(reinterpret_cast<T*>(h->cur_buf()), *P);
   delete P;
   MQ_LAUNCHED("k_diag");

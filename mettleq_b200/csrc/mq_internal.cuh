@@ -28,6 +28,22 @@ template <typename T> __device__ __forceinline__ T cmulc(T a, T b) {  // a * con
 }
 template <typename T, typename R> __device__ __forceinline__ T cscale(T a, R s) { a.x *= s; a.y *= s; return a; }
 
+// ---------------------------------------------------------------- async copies
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async(uint32_t dst, const void* src) {
+  if constexpr (BYTES == 8) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
+  } else {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+  }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // ---------------------------------------------------------------- limits
 constexpr int kMaxQubits = 32;        // 32-bit amplitude indices
 constexpr int kTileMaxC64 = 13;       // 2^13 complex64 = 64 KiB tile

@@ -36,11 +36,13 @@ struct PermParams {
   uint32_t tab[16];
 };
 
+// Persistent CTAs stream cosets through two shared-memory buffers: the input
+// coset of tile t+grid is fetched with cp.async while tile t is written out.
 template <typename R>
 __global__ void __launch_bounds__(256) k_perm(const V2<R>* __restrict__ in, V2<R>* __restrict__ out,
                                               const __grid_constant__ PermParams P) {
   using T = V2<R>;
-  __shared__ T buf[1024];
+  __shared__ __align__(16) T buf[2][1024];
   __shared__ uint32_t t_in[2][32], t_out[2][32], t_tab[2][32];
   const int tid = threadIdx.x;
   const int D = P.D;
@@ -58,22 +60,40 @@ __global__ void __launch_bounds__(256) k_perm(const V2<R>* __restrict__ in, V2<R
   __syncthreads();
   const uint32_t E = 1u << D;
   const uint32_t lomask = (1u << dlo) - 1u;
-  for (uint32_t tile = blockIdx.x; tile < P.n_tiles; tile += gridDim.x) {
-    uint32_t h_out = 0, h_in = P.c;
+  auto h_of = [&](uint32_t tile, bool input) -> uint32_t {
+    uint32_t h = input ? P.c : 0u;
     for (int k = 0; k < P.n_comp; ++k)
-      if ((tile >> k) & 1u) { h_out ^= P.comp_out[k]; h_in ^= P.comp_in[k]; }
-    __syncthreads();
-    for (uint32_t e = tid; e < E; e += blockDim.x) {
-      const uint32_t src = h_in ^ t_in[0][e & lomask] ^ t_in[1][e >> dlo];
-      buf[e] = in[src];
+      if ((tile >> k) & 1u) h ^= input ? P.comp_in[k] : P.comp_out[k];
+    return h;
+  };
+  uint32_t tile = blockIdx.x;
+  if (tile < P.n_tiles) {
+    const uint32_t h_in = h_of(tile, true);
+    for (uint32_t e = tid; e < E; e += blockDim.x)
+      cp_async<sizeof(T)>(smem_u32(&buf[0][e]), in + (h_in ^ t_in[0][e & lomask] ^ t_in[1][e >> dlo]));
+  }
+  cp_async_commit();
+  for (int it = 0; tile < P.n_tiles; tile += gridDim.x, ++it) {
+    const uint32_t next = tile + gridDim.x;
+    if (next < P.n_tiles) {
+      const uint32_t h_in = h_of(next, true);
+      T* nb = buf[(it + 1) & 1];
+      for (uint32_t e = tid; e < E; e += blockDim.x)
+        cp_async<sizeof(T)>(smem_u32(&nb[e]), in + (h_in ^ t_in[0][e & lomask] ^ t_in[1][e >> dlo]));
     }
+    cp_async_commit();
+    cp_async_wait<1>();
     __syncthreads();
+    const T* cb = buf[it & 1];
+    const uint32_t h_out = h_of(tile, false);
     for (uint32_t e = tid; e < E; e += blockDim.x) {
       const uint32_t y = h_out ^ t_out[0][e & lomask] ^ t_out[1][e >> dlo];
       const uint32_t slot = t_tab[0][e & lomask] ^ t_tab[1][e >> dlo];
-      out[y] = buf[slot];
+      out[y] = cb[slot];
     }
+    __syncthreads();
   }
+  cp_async_wait<0>();
 }
 
 // ------------------------------------------------------------ GF(2) algebra

@@ -76,6 +76,8 @@ class StateVector:
         N.check(lib.mq_state_create(self.n, self._dt, self.device, C.c_void_p(stream or 0), C.byref(h)))
         self._h = h
         self._lib = lib
+        # host->device parameter bytes handed to kernels (end-to-end accounting)
+        self.param_bytes = 0
 
     # -- lifetime -------------------------------------------------------
     def close(self) -> None:
@@ -146,6 +148,7 @@ class StateVector:
                 if not (0 <= int(q) < self.n):
                     raise ValueError("Qubit index out of range")
                 act[int(q)] = 1
+        self.param_bytes += m.nbytes + (act.nbytes if act is not None else 0)
         N.check(self._lib.mq_apply_u2_layer(self._h, _ptr(m), _ptr(act) if act is not None else None))
 
     def apply_u2_uniform(self, u2x2) -> None:
@@ -170,6 +173,7 @@ class StateVector:
             coff[i + 1] = len(ctl)
         controls = np.array(ctl if ctl else [0], dtype=np.int32)
         mats = _mats_array(len(gates), [np.asarray(u).reshape(4) for _, _, u in gates])
+        self.param_bytes += targets.nbytes + coff.nbytes + controls.nbytes + mats.nbytes
         N.check(self._lib.mq_apply_controlled_u2(self._h, len(gates), _ptr(targets), _ptr(coff), _ptr(controls),
                                                  _ptr(mats)))
 
@@ -189,6 +193,7 @@ class StateVector:
             wires[2 * i + 1] = int(b)
             pp = list(p)
             params[i, :len(pp)] = pp
+        self.param_bytes += kinds.nbytes + wires.nbytes + params.nbytes
         N.check(self._lib.mq_apply_diag_terms(self._h, k, _ptr(kinds), _ptr(wires), _ptr(params)))
 
     def apply_zz_weighted(self, bonds: Sequence[Tuple[int, int]], thetas: Sequence[float]) -> None:
@@ -208,6 +213,7 @@ class StateVector:
             return
         b = np.ascontiguousarray(np.asarray(bonds, dtype=np.int32).reshape(-1))
         t = np.ascontiguousarray(np.asarray(thetas, dtype=np.float64))
+        self.param_bytes += b.nbytes + t.nbytes
         N.check(self._lib.mq_apply_diag_layer(self._h, int(kind), len(bonds), _ptr(b), _ptr(t)))
 
     # -- (c) QFT ------------------------------------------------------------
@@ -225,6 +231,7 @@ class StateVector:
         r = np.ascontiguousarray(np.asarray([int(x) for x in rows], dtype=np.uint64))
         if r.size != self.n:
             raise ValueError("rows must have one mask per qubit")
+        self.param_bytes += r.nbytes + 8
         N.check(self._lib.mq_apply_xor_affine(self._h, _ptr(r), int(c)))
 
     # -- (e) probabilities, sampling, expectations ------------------------

@@ -100,37 +100,73 @@ def decompose(ops: Sequence[dict]) -> List[dict]:
     return out
 
 
+def _category(op: dict) -> str:
+    name = op["name"]
+    if len(op.get("wires", [])) == 1 and name != "_QFTSTAGE":
+        return "single"
+    if name in DIAG_TWO:
+        return "diag"
+    if name in AFFINE:
+        return "affine"
+    if name in CONTROLLED:
+        return "controlled"
+    return "other:" + name
+
+
 def dependency_schedule(ops: Sequence[dict]) -> List[dict]:
-    """Hoist ready single-qubit ops before ready multi-qubit ops without
-    changing any wire's op order (device.py:557-606)."""
+    """Topological re-order of the per-wire dependency DAG that exposes
+    fusable layers (device.py:557-606 hoists ready single-qubit ops).
+
+    Ops on the same wire keep their order; only ops on disjoint wires move.
+    Policy: keep extending the current multi-qubit run while ops of its
+    category are ready (so a CNOT ladder or a ZZ chain is not interrupted by
+    hoisted one-qubit gates), otherwise emit every ready one-qubit op,
+    otherwise start the category of the earliest ready op."""
+    import heapq
     count = len(ops)
     if count < 2:
         return list(ops)
     indeg = [0] * count
-    succ = [set() for _ in range(count)]
+    succ: List[List[int]] = [[] for _ in range(count)]
     last: Dict[int, int] = {}
     for i, op in enumerate(ops):
         preds = {last[w] for w in op.get("wires", []) if w in last}
         indeg[i] = len(preds)
         for p in preds:
-            succ[p].add(i)
+            succ[p].append(i)
         for w in op.get("wires", []):
             last[w] = i
-    ready = {i for i, d in enumerate(indeg) if d == 0}
+    cats = [_category(op) for op in ops]
+    ready: Dict[str, list] = {}
+    for i in range(count):
+        if indeg[i] == 0:
+            heapq.heappush(ready.setdefault(cats[i], []), i)
     out: List[dict] = []
-    while ready:
-        single = [i for i in ready if len(ops[i].get("wires", [])) == 1]
-        batch = sorted(single if single else ready)
-        for i in batch:
-            ready.remove(i)
-            out.append(ops[i])
-        for i in batch:
-            for s in succ[i]:
-                indeg[s] -= 1
-                if indeg[s] == 0:
-                    ready.add(s)
-    if len(out) != count:
-        raise RuntimeError("operation dependency graph contains a cycle")
+    current: Optional[str] = None
+
+    def emit(i):
+        out.append(ops[i])
+        for s_ in succ[i]:
+            indeg[s_] -= 1
+            if indeg[s_] == 0:
+                heapq.heappush(ready.setdefault(cats[s_], []), s_)
+
+    while len(out) < count:
+        if current is not None and ready.get(current):
+            batch = [heapq.heappop(ready[current]) for _ in range(len(ready[current]))]
+            for i in batch:
+                emit(i)
+            continue
+        if ready.get("single"):
+            batch = [heapq.heappop(ready["single"]) for _ in range(len(ready["single"]))]
+            for i in batch:
+                emit(i)
+            current = None
+            continue
+        nonempty = [(h[0], c) for c, h in ready.items() if h]
+        if not nonempty:
+            raise RuntimeError("operation dependency graph contains a cycle")
+        current = min(nonempty)[1]
     return out
 
 
@@ -257,9 +293,30 @@ def _qft_inverse_stage(ops, i):
     return None
 
 
+def _mark_qft_stages(ops: List[dict]) -> List[dict]:
+    """Replace forward / inverse QFT stage patterns by _QFTSTAGE pseudo-ops
+    (wires = the stage's subregister) before any re-ordering."""
+    out: List[dict] = []
+    i, N = 0, len(ops)
+    while i < N:
+        st = _qft_forward_stage(ops, i)
+        inv = False
+        if st is None:
+            st = _qft_inverse_stage(ops, i)
+            inv = st is not None
+        if st is not None:
+            j, m, nxt = st
+            out.append({"name": "_QFTSTAGE", "j": j, "m": m, "inverse": inv, "wires": list(range(j, m))})
+            i = nxt
+            continue
+        out.append(ops[i])
+        i += 1
+    return out
+
+
 def fuse(operations: Sequence[dict], n: int, *, schedule: bool = True) -> List[Dict[str, Any]]:
-    ops = decompose(normalize(operations, n))
-    if schedule and any(op["name"] in ("U2", "U3") for op in ops):
+    ops = _mark_qft_stages(decompose(normalize(operations, n)))
+    if schedule:
         ops = dependency_schedule(ops)
     fused: List[Dict[str, Any]] = []
     i = 0
@@ -267,25 +324,14 @@ def fuse(operations: Sequence[dict], n: int, *, schedule: bool = True) -> List[D
     while i < N:
         op = ops[i]
         name = op["name"]
-        st = _qft_forward_stage(ops, i)
-        if st is not None:
-            j, m, nxt = st
-            fused.append({"name": "_QFTSTAGE", "j": j, "m": m, "inverse": False})
-            i = nxt
-            continue
-        st = _qft_inverse_stage(ops, i)
-        if st is not None:
-            j, m, nxt = st
-            fused.append({"name": "_QFTSTAGE", "j": j, "m": m, "inverse": True})
-            i = nxt
+        if name == "_QFTSTAGE":
+            fused.append({k: op[k] for k in ("name", "j", "m", "inverse")})
+            i += 1
             continue
         if len(op.get("wires", [])) == 1:
             j = i
             per_wire: Dict[int, np.ndarray] = {}
-            while j < N and len(ops[j].get("wires", [])) == 1:
-                # stop before an H that opens a QFT stage
-                if j > i and (_qft_forward_stage(ops, j) is not None):
-                    break
+            while j < N and len(ops[j].get("wires", [])) == 1 and ops[j]["name"] != "_QFTSTAGE":
                 q = ops[j]["wires"][0]
                 per_wire[q] = _single_matrix(ops[j]) @ per_wire.get(q, _EYE)
                 j += 1
