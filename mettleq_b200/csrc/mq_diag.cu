@@ -40,7 +40,9 @@ struct DiagParams {
   uint32_t n_pairs;  // 2^(n-1) element pairs
   int32_t n_luts;
   uint32_t n_entries;
-  int32_t n_low;     // tables [0, n_low) read index bits 0-2
+  int32_t n_low;     // tables [0, n_low) read index bit 0
+  int32_t pair_lut0; // table 0 is a contiguous window starting at bit 0
+  int32_t pad[3];
   DiagLut lut[kMaxLuts];
   V2<R> e[DiagCap<R>::v];
 };
@@ -52,10 +54,11 @@ __device__ __forceinline__ uint32_t lut_index(const DiagLut& L, uint32_t i) {
   return x;
 }
 
-// Each thread handles aligned groups of 8 consecutive amplitudes (index bits
-// 0-2 vary inside a group).  Tables [0, n_low) read index bits 0-2 and are
-// looked up per amplitude; the product of the remaining tables is the same
-// for the whole group and is computed once.
+// Each thread handles amplitude pairs (2p, 2p+1), four independent pairs per
+// iteration, with 16-byte (complex64) accesses that are contiguous across the
+// warp.  Tables [0, n_low) read index bit 0: when table 0 is a window starting
+// at bit 0 (pair_lut0) the pair's two entries are adjacent and read as one
+// 16-byte value; the other tables give one factor per pair.
 template <typename R>
 __global__ void __launch_bounds__(256) k_diag(V2<R>* __restrict__ st, const __grid_constant__ DiagParams<R> P) {
   using T = V2<R>;
@@ -63,47 +66,52 @@ __global__ void __launch_bounds__(256) k_diag(V2<R>* __restrict__ st, const __gr
   T* lut = reinterpret_cast<T*>(smem_raw);
   for (uint32_t j = threadIdx.x; j < P.n_entries; j += blockDim.x) lut[j] = P.e[j];
   __syncthreads();
-  const uint32_t n_groups = P.n_pairs >> 2;  // groups of 8 (n >= 3)
+  constexpr int U = 4;
   const uint32_t stride = gridDim.x * blockDim.x;
   const int n_low = P.n_low;
-  for (uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x; gi < n_groups; gi += stride) {
-    const uint32_t i0 = gi << 3;
-    T a[8];
-    if constexpr (sizeof(R) == 4) {
-      const float4* p4 = reinterpret_cast<const float4*>(st + i0);
+  const bool pair0 = P.pair_lut0;
+  for (uint32_t p0 = blockIdx.x * blockDim.x + threadIdx.x; p0 < P.n_pairs; p0 += U * stride) {
+    T a0[U], a1[U];
 #pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const float4 x = p4[v];
-        a[2 * v] = make_float2(x.x, x.y);
-        a[2 * v + 1] = make_float2(x.z, x.w);
+    for (int u = 0; u < U; ++u) {
+      const uint32_t p = p0 + (uint32_t)u * stride;
+      if (p < P.n_pairs) {
+        if constexpr (sizeof(R) == 4) {
+          const float4 x = reinterpret_cast<const float4*>(st)[p];
+          a0[u] = make_float2(x.x, x.y);
+          a1[u] = make_float2(x.z, x.w);
+        } else {
+          a0[u] = st[2 * p];
+          a1[u] = st[2 * p + 1];
+        }
       }
-    } else {
-#pragma unroll
-      for (int v = 0; v < 8; ++v) a[v] = st[i0 + v];
     }
-    T hi = mk<R>(1, 0);
-    for (int l = n_low; l < P.n_luts; ++l) hi = cmul(hi, lut[P.lut[l].off + lut_index(P.lut[l], i0)]);
 #pragma unroll
-    for (int v = 0; v < 8; ++v) {
-      T f = hi;
-      for (int l = 0; l < n_low; ++l) f = cmul(f, lut[P.lut[l].off + lut_index(P.lut[l], i0 + v)]);
-      a[v] = cmul(a[v], f);
-    }
-    if constexpr (sizeof(R) == 4) {
-      float4* p4 = reinterpret_cast<float4*>(st + i0);
-#pragma unroll
-      for (int v = 0; v < 4; ++v) p4[v] = make_float4(a[2 * v].x, a[2 * v].y, a[2 * v + 1].x, a[2 * v + 1].y);
-    } else {
-#pragma unroll
-      for (int v = 0; v < 8; ++v) st[i0 + v] = a[v];
-    }
-  }
-  // states of fewer than 8 amplitudes
-  if (n_groups == 0 && blockIdx.x == 0) {
-    for (uint32_t i = threadIdx.x; i < 2 * P.n_pairs; i += blockDim.x) {
-      T f = mk<R>(1, 0);
-      for (int l = 0; l < P.n_luts; ++l) f = cmul(f, lut[P.lut[l].off + lut_index(P.lut[l], i)]);
-      st[i] = cmul(st[i], f);
+    for (int u = 0; u < U; ++u) {
+      const uint32_t p = p0 + (uint32_t)u * stride;
+      if (p >= P.n_pairs) continue;
+      const uint32_t i0 = 2 * p;
+      T hi = mk<R>(1, 0);
+      for (int l = n_low; l < P.n_luts; ++l) hi = cmul(hi, lut[P.lut[l].off + lut_index(P.lut[l], i0)]);
+      T f0 = hi, f1 = hi;
+      int l = 0;
+      if (pair0 && n_low > 0) {
+        const uint32_t k = P.lut[0].off + lut_index(P.lut[0], i0);
+        f0 = cmul(f0, lut[k]);
+        f1 = cmul(f1, lut[k + 1]);
+        l = 1;
+      }
+      for (; l < n_low; ++l) {
+        f0 = cmul(f0, lut[P.lut[l].off + lut_index(P.lut[l], i0)]);
+        f1 = cmul(f1, lut[P.lut[l].off + lut_index(P.lut[l], i0 + 1)]);
+      }
+      const T b0 = cmul(a0[u], f0), b1 = cmul(a1[u], f1);
+      if constexpr (sizeof(R) == 4) {
+        reinterpret_cast<float4*>(st)[p] = make_float4(b0.x, b0.y, b1.x, b1.y);
+      } else {
+        st[i0] = b0;
+        st[i0 + 1] = b1;
+      }
     }
   }
 }
@@ -235,16 +243,21 @@ template <typename R>
 static int launch_diag_pass(mq_state* h, const std::vector<PlannedLut>& in_luts) {
   using T = V2<R>;
   std::vector<PlannedLut> luts;
+  auto has0 = [](const PlannedLut& L) { return std::find(L.pos.begin(), L.pos.end(), 0) != L.pos.end(); };
   for (const auto& L : in_luts)
-    if (!L.pos.empty() && *std::min_element(L.pos.begin(), L.pos.end()) < 3) luts.push_back(L);
+    if (has0(L) && L.contig && L.pos[0] == 0) luts.push_back(L);
+  const bool pair0 = !luts.empty();
+  for (const auto& L : in_luts)
+    if (has0(L) && !(L.contig && L.pos[0] == 0)) luts.push_back(L);
   const int n_low = (int)luts.size();
   for (const auto& L : in_luts)
-    if (L.pos.empty() || *std::min_element(L.pos.begin(), L.pos.end()) >= 3) luts.push_back(L);
+    if (!has0(L)) luts.push_back(L);
   auto* P = new DiagParams<R>();
   std::memset(P, 0, sizeof(DiagParams<R>));
   P->n_pairs = (uint32_t)(h->dim() >> 1);
   P->n_luts = (int32_t)luts.size();
   P->n_low = n_low;
+  P->pair_lut0 = pair0 ? 1 : 0;
   uint32_t off = 0;
   for (size_t l = 0; l < luts.size(); ++l) {
     const PlannedLut& L = luts[l];
@@ -258,8 +271,8 @@ static int launch_diag_pass(mq_state* h, const std::vector<PlannedLut>& in_luts)
   }
   P->n_entries = off;
   const size_t smem = sizeof(T) * std::max<uint32_t>(off, 1);
-  const uint32_t groups = std::max<uint32_t>(1, P->n_pairs >> 2);
-  const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((groups + 255) / 256, (uint64_t)h->num_sms * 8));
+  const uint32_t pairs = P->n_pairs;
+  const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((pairs + 255) / 256, (uint64_t)h->num_sms * 8));
   k_diag<R><<<grid, 256, smem, h->stream>>>(reinterpret_cast<T*>(h->cur_buf()), *P);
   delete P;
   MQ_LAUNCHED("k_diag");

@@ -38,58 +38,75 @@ struct PermParams {
 
 // Persistent CTAs stream cosets through two shared-memory buffers: the input
 // coset of tile t+grid is fetched with cp.async while tile t is written out.
-template <typename R>
+// Tile elements e = tid + NT*j.  All index maps are GF(2)-linear in e, so a
+// thread's lane/warp part is combined once and each element adds one
+// CTA-uniform term.  Only basis vector 0 (= e_0) has index bit 0 set, so
+// input pairs (e, e^1) are one aligned 16-byte chunk, stored in shared
+// memory with the coset's bit-0 offset `flip` folded into the slot index.
+template <typename R, int D>
 __global__ void __launch_bounds__(256) k_perm(const V2<R>* __restrict__ in, V2<R>* __restrict__ out,
                                               const __grid_constant__ PermParams P) {
   using T = V2<R>;
-  __shared__ __align__(16) T buf[2][1024];
-  __shared__ uint32_t t_in[2][32], t_out[2][32], t_tab[2][32];
+  constexpr int E = 1 << D;
+  constexpr int NT = E < 256 ? E : 256;
+  constexpr int EPT = E / NT;
+  constexpr bool PAIRS = (sizeof(T) == 8) && D >= 1;  // 16-byte input chunks
+  constexpr int CPT = PAIRS ? (EPT >= 2 ? EPT / 2 : 1) : EPT;
+  __shared__ __align__(16) T buf[2][E < 2 ? 2 : E];
+  __shared__ uint32_t t_in[E], t_out[E], t_tab[E];
   const int tid = threadIdx.x;
-  const int D = P.D;
-  const int dlo = D < 5 ? D : 5;
-  const int dhi = D - dlo;
-  if (tid < 32) {
-    uint32_t a = 0, b = 0, c = 0, x = 0, y = 0, z = 0;
-    for (int k = 0; k < dlo; ++k)
-      if (tid & (1 << k)) { a ^= P.lin_in[k]; b ^= P.lin_out[k]; c ^= P.tab[k]; }
-    for (int k = 0; k < dhi; ++k)
-      if (tid & (1 << k)) { x ^= P.lin_in[dlo + k]; y ^= P.lin_out[dlo + k]; z ^= P.tab[dlo + k]; }
-    t_in[0][tid] = a; t_out[0][tid] = b; t_tab[0][tid] = c;
-    t_in[1][tid] = x; t_out[1][tid] = y; t_tab[1][tid] = z;
+  // full linear tables over the D tile coordinates (E <= 1024 entries)
+  for (int e = tid; e < E; e += NT) {
+    uint32_t a = 0, b = 0, c = 0;
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+      if (e & (1 << k)) { a ^= P.lin_in[k]; b ^= P.lin_out[k]; c ^= P.tab[k]; }
+    t_in[e] = a; t_out[e] = b; t_tab[e] = c;
   }
   __syncthreads();
-  const uint32_t E = 1u << D;
-  const uint32_t lomask = (1u << dlo) - 1u;
   auto h_of = [&](uint32_t tile, bool input) -> uint32_t {
     uint32_t h = input ? P.c : 0u;
     for (int k = 0; k < P.n_comp; ++k)
       if ((tile >> k) & 1u) h ^= input ? P.comp_in[k] : P.comp_out[k];
     return h;
   };
-  uint32_t tile = blockIdx.x;
-  if (tile < P.n_tiles) {
+  // per-thread parts: input chunks c = tid + NT*j cover elements 2c, 2c+1
+  auto issue = [&](uint32_t tile, int which) {
     const uint32_t h_in = h_of(tile, true);
-    for (uint32_t e = tid; e < E; e += blockDim.x)
-      cp_async<sizeof(T)>(smem_u32(&buf[0][e]), in + (h_in ^ t_in[0][e & lomask] ^ t_in[1][e >> dlo]));
-  }
+    const uint32_t sb = smem_u32(&buf[which][0]);
+    if constexpr (PAIRS) {
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        const uint32_t c = (uint32_t)tid + (uint32_t)(NT * j);
+        if (2 * c < (uint32_t)E) {
+          const uint32_t src = (h_in ^ t_in[2 * c]) & ~1u;
+          cp_async<16>(sb + 16u * c, in + src);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < EPT; ++j) {
+        const uint32_t e = (uint32_t)tid + (uint32_t)(NT * j);
+        cp_async<sizeof(T)>(sb + (uint32_t)sizeof(T) * e, in + (h_in ^ t_in[e]));
+      }
+    }
+  };
+  uint32_t tile = blockIdx.x;
+  if (tile < P.n_tiles) issue(tile, 0);
   cp_async_commit();
   for (int it = 0; tile < P.n_tiles; tile += gridDim.x, ++it) {
     const uint32_t next = tile + gridDim.x;
-    if (next < P.n_tiles) {
-      const uint32_t h_in = h_of(next, true);
-      T* nb = buf[(it + 1) & 1];
-      for (uint32_t e = tid; e < E; e += blockDim.x)
-        cp_async<sizeof(T)>(smem_u32(&nb[e]), in + (h_in ^ t_in[0][e & lomask] ^ t_in[1][e >> dlo]));
-    }
+    if (next < P.n_tiles) issue(next, (it + 1) & 1);
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
     const T* cb = buf[it & 1];
     const uint32_t h_out = h_of(tile, false);
-    for (uint32_t e = tid; e < E; e += blockDim.x) {
-      const uint32_t y = h_out ^ t_out[0][e & lomask] ^ t_out[1][e >> dlo];
-      const uint32_t slot = t_tab[0][e & lomask] ^ t_tab[1][e >> dlo];
-      out[y] = cb[slot];
+    const uint32_t flip = PAIRS ? (h_of(tile, true) & 1u) : 0u;
+#pragma unroll
+    for (int j = 0; j < EPT; ++j) {
+      const uint32_t e = (uint32_t)tid + (uint32_t)(NT * j);
+      out[h_out ^ t_out[e]] = cb[t_tab[e] ^ flip];
     }
     __syncthreads();
   }
@@ -165,13 +182,35 @@ bool gf2_invert(int n, const uint32_t* cols, uint32_t* inv_cols) {
   return true;
 }
 
-template <typename R>
-static int launch_perm_t(mq_state* h, const PermParams& P) {
+template <typename R, int D>
+static int launch_perm_d(mq_state* h, const PermParams& P) {
+  constexpr int E = 1 << D;
+  constexpr int NT = E < 256 ? E : 256;
   const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(P.n_tiles, (uint64_t)h->num_sms * 8));
   const V2<R>* src = reinterpret_cast<const V2<R>*>(h->buf[h->cur]);
   V2<R>* dst = reinterpret_cast<V2<R>*>(h->buf[1 - h->cur]);
-  k_perm<R><<<grid, 256, 0, h->stream>>>(src, dst, P);
+  k_perm<R, D><<<grid, NT, 0, h->stream>>>(src, dst, P);
   MQ_LAUNCHED("k_perm");
+  return MQ_OK;
+}
+
+template <typename R>
+static int launch_perm_t(mq_state* h, const PermParams& P) {
+  int rc = MQ_EUNSUPPORTED;
+  switch (P.D) {
+    case 1: rc = launch_perm_d<R, 1>(h, P); break;
+    case 2: rc = launch_perm_d<R, 2>(h, P); break;
+    case 3: rc = launch_perm_d<R, 3>(h, P); break;
+    case 4: rc = launch_perm_d<R, 4>(h, P); break;
+    case 5: rc = launch_perm_d<R, 5>(h, P); break;
+    case 6: rc = launch_perm_d<R, 6>(h, P); break;
+    case 7: rc = launch_perm_d<R, 7>(h, P); break;
+    case 8: rc = launch_perm_d<R, 8>(h, P); break;
+    case 9: rc = launch_perm_d<R, 9>(h, P); break;
+    case 10: rc = launch_perm_d<R, 10>(h, P); break;
+    default: return fail(MQ_EUNSUPPORTED, "permutation tile size not instantiated");
+  }
+  if (rc) return rc;
   h->cur = 1 - h->cur;
   h->launches += 1;
   h->sweeps += 1;
@@ -206,6 +245,18 @@ int launch_affine_cols(mq_state* h, const uint32_t* cols, uint32_t c) {
     if ((int)vout.size() < D && eout.add(w, (int)vout.size())) vout.push_back(w);
   }
   if ((int)vin.size() != D || (int)vout.size() != D) return fail(MQ_EDEVICE, "affine tile basis construction failed");
+  // Clear index bit 0 from every basis vector but the first (which is e_0),
+  // so that tile coordinate 0 alone decides the bit-0 parity of an address.
+  if (pas >= 1) {
+    Echelon e2in, e2out;
+    for (int k = 1; k < D; ++k) {
+      if (vin[k] & 1u) vin[k] ^= vin[0];
+      if (vout[k] & 1u) vout[k] ^= vout[0];
+    }
+    for (int k = 0; k < D; ++k) { e2in.add(vin[k], k); e2out.add(vout[k], k); }
+    ein = e2in;
+    eout = e2out;
+  }
   PermParams P;
   std::memset(&P, 0, sizeof(P));
   P.n = (uint8_t)n;

@@ -15,9 +15,9 @@
 //   * the tile is processed in place in shared memory by "phases": each
 //     thread loads 2^LR amplitudes that differ in LR tile bits into
 //     registers, applies the gates of those bits, and writes them back;
-//   * shared-memory addresses are XOR-swizzled with a per-sweep linear map
-//     chosen on the host so that every phase's accesses are free of bank
-//     conflicts;
+//   * global memory moves in 16-byte chunks, loaded with cp.async and stored
+//     with vector stores, in a tile-local = shared-memory index layout, so
+//     all load/store offsets are compile-time immediates;
 //   * the finished tile is written back with coalesced stores.
 //
 // QFT stages (sim.py:522-563, no final swaps): stage j on index bit s is a
@@ -27,6 +27,7 @@
 // in the required order (high bit first forward, low bit first inverse); the
 // 1/sqrt(2) of every butterfly is applied once per sweep as 2^{-stages/2}.
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -41,31 +42,40 @@ enum : uint8_t { OP_U2 = 0, OP_QFT_FWD = 1, OP_QFT_INV = 2, OP_CU2 = 3 };
 
 constexpr int kMaxPhases = 6;
 constexpr int kMaxOps = 16;
-constexpr int kMaxTileBits = 12;
+constexpr int kMaxTileBits = 13;
 
 struct TileOp {
   uint8_t kind, phase, rk, lad_shift, width, pad[3];
   uint32_t cmask;  // OP_CU2: global index bits that must all be set
   uint32_t pad2;
   double u[8];     // 2x2 matrix (re, im interleaved)
-  float uf[8];     // the same matrix rounded to float for complex64 sweeps
 };
 
-struct PhaseDesc {
-  uint16_t swz_reg[5];               // swizzled smem offset of each register bit
-  uint16_t swz_grp[kMaxTileBits];    // ... of each group (thread/loop) bit
-  uint32_t g_reg[5];                 // global index bit of each register bit
+// One register phase: which tile bits sit in registers, the shared-memory
+// (tile-local) and global offsets of every register / group bit, and for
+// U(2) sweeps one matrix slot per register bit.
+struct __align__(16) PhaseDesc {
+  uint32_t s_reg[5];
+  uint32_t s_grp[kMaxTileBits];
+  uint32_t g_reg[5];
   uint32_t g_grp[kMaxTileBits];
+  uint32_t cmask[5];     // controls of the slot's gate (0 = none)
+  uint8_t active;        // slots carrying a gate
+  uint8_t any_ctl;       // some slot is controlled
+  alignas(16) float uf[5][8];   // rows read as two 16-byte vectors
+  alignas(16) double ud[5][8];
 };
+static_assert(offsetof(PhaseDesc, uf) % 16 == 0, "matrix rows must be 16-byte aligned");
+static_assert(sizeof(PhaseDesc) % 16 == 0, "PhaseDesc array stride must keep rows aligned");
 
 struct TileParams {
   uint32_t n_tiles;
   uint8_t n, m, n_phases, n_ops;
   uint8_t tile_bit[16];
-  uint8_t need_tw, has_scale, pad[6];
+  uint8_t need_tw, has_scale, hi_contig, hi_shift;
+  uint32_t pad2;
   double scale;
-  uint16_t swz_tile[16];             // swizzled smem offset of tile bit k
-  uint8_t ph_op[kMaxPhases + 2];     // ops of phase p are [ph_op[p], ph_op[p+1])
+  uint8_t ph_op[kMaxPhases + 2];     // QFT: ops of phase p are [ph_op[p], ph_op[p+1])
   PhaseDesc ph[kMaxPhases];
   TileOp ops[kMaxOps];
 };
@@ -90,7 +100,7 @@ template <> struct Twiddle<double> {
 };
 
 template <int LR>
-__device__ __forceinline__ uint32_t gsel(int r, const uint32_t* g) {
+__device__ __forceinline__ uint32_t osel(int r, const uint32_t* g) {
   uint32_t o = 0;
 #pragma unroll
   for (int k = 0; k < LR; ++k)
@@ -98,85 +108,97 @@ __device__ __forceinline__ uint32_t gsel(int r, const uint32_t* g) {
   return o;
 }
 
-// XOR of the swizzled shared-memory offsets of the set register bits
-// (swizzled offsets are multi-bit, so they combine with XOR, not OR).
-template <int LR>
-__device__ __forceinline__ uint32_t xsel(int r, const uint32_t* s) {
-  uint32_t o = 0;
-#pragma unroll
-  for (int k = 0; k < LR; ++k)
-    if (r & (1 << k)) o ^= s[k];
-  return o;
+// out = u0 * x0 + u1 * x1 as explicit fused multiply-adds (4 per component).
+template <typename T>
+__device__ __forceinline__ T cmac2(T u0, T x0, T u1, T x1) {
+  T r;
+  r.x = fma(u0.x, x0.x, fma(-u0.y, x0.y, fma(u1.x, x1.x, -u1.y * x1.y)));
+  r.y = fma(u0.x, x0.y, fma(u0.y, x0.x, fma(u1.x, x1.y, u1.y * x1.x)));
+  return r;
 }
 
-template <typename R, int LR, int K, bool QFT>
-__device__ __forceinline__ void apply_op_k(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const uint32_t* greg,
-                                           const float2* tw) {
+// 2x2 gate on register bit K; CTL: only where all cmask bits are set.
+template <typename R, int LR, int K, bool CTL>
+__device__ __forceinline__ void apply_u2(V2<R> (&a)[1 << LR], const PhaseDesc& D, uint32_t gq, const uint32_t* greg) {
   using T = V2<R>;
   constexpr int NR = 1 << LR;
-  if constexpr (!QFT) {
-    T u00, u01, u10, u11;
-    if constexpr (sizeof(R) == 4) {
-      u00 = mk<R>(op.uf[0], op.uf[1]); u01 = mk<R>(op.uf[2], op.uf[3]);
-      u10 = mk<R>(op.uf[4], op.uf[5]); u11 = mk<R>(op.uf[6], op.uf[7]);
-    } else {
-      u00 = mk<R>(op.u[0], op.u[1]); u01 = mk<R>(op.u[2], op.u[3]);
-      u10 = mk<R>(op.u[4], op.u[5]); u11 = mk<R>(op.u[6], op.u[7]);
-    }
-    const uint32_t cm = op.cmask;
-    const bool ctl = op.kind == OP_CU2;
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      if (r & (1 << K)) continue;
-      if (ctl && (((gq | gsel<LR>(r, greg)) & cm) != cm)) continue;
-      const T x0 = a[r], x1 = a[r | (1 << K)];
-      a[r] = cadd(cmul(u00, x0), cmul(u01, x1));
-      a[r | (1 << K)] = cadd(cmul(u10, x0), cmul(u11, x1));
-    }
+  T u00, u01, u10, u11;
+  if constexpr (sizeof(R) == 4) {
+    const float4 m0 = *reinterpret_cast<const float4*>(&D.uf[K][0]);
+    const float4 m1 = *reinterpret_cast<const float4*>(&D.uf[K][4]);
+    u00 = make_float2(m0.x, m0.y); u01 = make_float2(m0.z, m0.w);
+    u10 = make_float2(m1.x, m1.y); u11 = make_float2(m1.z, m1.w);
   } else {
-    const int width = op.width;
-    const int shift = op.lad_shift;
-    const uint32_t mask = width ? ((width >= 32) ? 0xffffffffu : ((1u << width) - 1u)) : 0u;
-    const bool fwd = op.kind == OP_QFT_FWD;
+    u00 = mk<R>(D.ud[K][0], D.ud[K][1]); u01 = mk<R>(D.ud[K][2], D.ud[K][3]);
+    u10 = mk<R>(D.ud[K][4], D.ud[K][5]); u11 = mk<R>(D.ud[K][6], D.ud[K][7]);
+  }
+  const uint32_t cm = D.cmask[K];
 #pragma unroll
-    for (int r = 0; r < NR; ++r) {
-      if (r & (1 << K)) continue;
-      const int r1 = r | (1 << K);
-      T x0 = a[r], x1 = a[r1];
-      uint32_t L = 0;
-      if (width) L = ((gq | gsel<LR>(r1, greg)) >> shift) & mask;
-      if (fwd) {
-        T d = csub(x0, x1);
-        a[r] = cadd(x0, x1);
-        if (L) d = cmul(d, Twiddle<R>::get(tw, L, width));
-        a[r1] = d;
-      } else {
-        if (L) x1 = cmulc(x1, Twiddle<R>::get(tw, L, width));
-        a[r] = cadd(x0, x1);
-        a[r1] = csub(x0, x1);
-      }
+  for (int r = 0; r < NR; ++r) {
+    if (r & (1 << K)) continue;
+    if (CTL && (((gq | osel<LR>(r, greg)) & cm) != cm)) continue;
+    const T x0 = a[r], x1 = a[r | (1 << K)];
+    a[r] = cmac2(u00, x0, u01, x1);
+    a[r | (1 << K)] = cmac2(u10, x0, u11, x1);
+  }
+}
+
+template <typename R, int LR, bool CTL>
+__device__ __forceinline__ void apply_u2_phase(V2<R> (&a)[1 << LR], const PhaseDesc& D, uint32_t gq,
+                                               const uint32_t* greg) {
+  const uint32_t act = D.active;
+  if (act & 1u) apply_u2<R, LR, 0, CTL>(a, D, gq, greg);
+  if constexpr (LR > 1) if (act & 2u) apply_u2<R, LR, 1, CTL>(a, D, gq, greg);
+  if constexpr (LR > 2) if (act & 4u) apply_u2<R, LR, 2, CTL>(a, D, gq, greg);
+  if constexpr (LR > 3) if (act & 8u) apply_u2<R, LR, 3, CTL>(a, D, gq, greg);
+  if constexpr (LR > 4) if (act & 16u) apply_u2<R, LR, 4, CTL>(a, D, gq, greg);
+}
+
+// One QFT stage on register bit K (forward: butterfly then phase; inverse:
+// conjugate phase then butterfly).
+template <typename R, int LR, int K>
+__device__ __forceinline__ void apply_qft(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const uint32_t* greg,
+                                          const float2* tw) {
+  using T = V2<R>;
+  constexpr int NR = 1 << LR;
+  const int width = op.width;
+  const int shift = op.lad_shift;
+  const uint32_t mask = width ? ((width >= 32) ? 0xffffffffu : ((1u << width) - 1u)) : 0u;
+  const bool fwd = op.kind == OP_QFT_FWD;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) {
+    if (r & (1 << K)) continue;
+    const int r1 = r | (1 << K);
+    T x0 = a[r], x1 = a[r1];
+    uint32_t L = 0;
+    if (width) L = ((gq | osel<LR>(r1, greg)) >> shift) & mask;
+    if (fwd) {
+      T d = csub(x0, x1);
+      a[r] = cadd(x0, x1);
+      if (L) d = cmul(d, Twiddle<R>::get(tw, L, width));
+      a[r1] = d;
+    } else {
+      if (L) x1 = cmulc(x1, Twiddle<R>::get(tw, L, width));
+      a[r] = cadd(x0, x1);
+      a[r1] = csub(x0, x1);
     }
   }
 }
 
-template <typename R, int LR, bool QFT>
-__device__ __forceinline__ void apply_op(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const uint32_t* greg,
-                                         const float2* tw) {
+template <typename R, int LR>
+__device__ __forceinline__ void apply_qft_op(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const uint32_t* greg,
+                                             const float2* tw) {
   switch (op.rk) {
-    case 0: apply_op_k<R, LR, 0, QFT>(a, op, gq, greg, tw); break;
-    case 1: if constexpr (LR > 1) apply_op_k<R, LR, 1, QFT>(a, op, gq, greg, tw); break;
-    case 2: if constexpr (LR > 2) apply_op_k<R, LR, 2, QFT>(a, op, gq, greg, tw); break;
-    case 3: if constexpr (LR > 3) apply_op_k<R, LR, 3, QFT>(a, op, gq, greg, tw); break;
-    case 4: if constexpr (LR > 4) apply_op_k<R, LR, 4, QFT>(a, op, gq, greg, tw); break;
+    case 0: apply_qft<R, LR, 0>(a, op, gq, greg, tw); break;
+    case 1: if constexpr (LR > 1) apply_qft<R, LR, 1>(a, op, gq, greg, tw); break;
+    case 2: if constexpr (LR > 2) apply_qft<R, LR, 2>(a, op, gq, greg, tw); break;
+    case 3: if constexpr (LR > 3) apply_qft<R, LR, 3>(a, op, gq, greg, tw); break;
+    case 4: if constexpr (LR > 4) apply_qft<R, LR, 4>(a, op, gq, greg, tw); break;
     default: break;
   }
 }
 
-// Tile of 2^M amplitudes, 2^LT threads, 2^LR amplitudes in registers per
-// group, 2^(M-LR-LT) groups per thread per phase.  QFT selects the op family
-// (QFT stages vs U(2) / controlled U(2)) so each instance carries only the
-// code it runs.
-template <typename R, int M, int LR, int LT>
+template <int M>
 __device__ __forceinline__ uint32_t tile_base_of(uint32_t tile, const TileParams& P) {
   uint64_t x = tile;
 #pragma unroll
@@ -187,22 +209,35 @@ __device__ __forceinline__ uint32_t tile_base_of(uint32_t tile, const TileParams
   return (uint32_t)x;
 }
 
+// Tile of 2^M amplitudes in an identity shared-memory layout (tile-local
+// index = shared-memory index), 2^LT threads, 2^LR amplitudes per register
+// group.  Global traffic moves in 16-byte chunks (two complex64 or one
+// complex128 amplitude): chunk c covers tile-local element c << CB.
 template <typename R, int M, int LR, int LT, bool QFT>
-__global__ void __launch_bounds__(1 << LT, (LT >= 7 ? 3 : 1))
+__global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? 2 : (LT >= 7 ? 3 : 1))))
 k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
   using T = V2<R>;
   constexpr int NT = 1 << LT;
   constexpr int NR = 1 << LR;
   constexpr int E = 1 << M;
   constexpr int GPT = (E / NR) / NT;
-  constexpr int LPT = E / NT;            // elements per thread in load / store
-  constexpr int LHI = M - LT;            // element-index bits above the thread bits
-  constexpr int CPB = sizeof(T);         // bytes per cp.async
-  static_assert(GPT >= 1 && LPT >= 1, "bad tile configuration");
+  constexpr int CB = sizeof(T) == 8 ? 1 : 0;          // log2 amplitudes per 16-byte chunk
+  constexpr int NCH = E >> CB;                         // chunks per tile
+  constexpr int CPT = NCH / NT;                        // chunks per thread
+  constexpr int LCH = (M - CB) - LT;                   // chunk-index bits above the thread bits
+  static_assert(GPT >= 1 && CPT >= 1, "bad tile configuration");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* bufs = reinterpret_cast<T*>(smem_raw);
-  float2* tw = reinterpret_cast<float2*>(smem_raw + 2 * sizeof(T) * E);
+  PhaseDesc* phs = reinterpret_cast<PhaseDesc*>(smem_raw + 2 * sizeof(T) * E);
+  float2* tw = reinterpret_cast<float2*>(smem_raw + 2 * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases);
   const int tid = threadIdx.x;
+  {
+    const uint32_t words = (uint32_t)(sizeof(PhaseDesc) * P.n_phases / 4);
+    const uint32_t* srcw = reinterpret_cast<const uint32_t*>(&P.ph[0]);
+    uint32_t* dstw = reinterpret_cast<uint32_t*>(phs);
+    for (uint32_t w = tid; w < words; w += NT) dstw[w] = srcw[w];
+  }
+  __syncthreads();
 
   if (QFT && P.need_tw) {
     for (int j = tid; j < 3072; j += NT) {
@@ -215,24 +250,28 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
     }
   }
 
-  // per-thread part of the load/store mapping (element e = tid + k*NT)
-  uint32_t g_t = 0, s_t = 0;
+  // chunk c = tid + k*NT: global part of the thread bits, computed once
+  uint32_t g_t = 0;
 #pragma unroll
   for (int b = 0; b < LT; ++b)
-    if ((tid >> b) & 1) { g_t |= 1u << P.tile_bit[b]; s_t ^= P.swz_tile[b]; }
+    if ((tid >> b) & 1) g_t |= 1u << P.tile_bit[CB + b];
+  const bool hi_contig = P.hi_contig;
+  const int hi_shift = P.hi_shift;
+  auto g_k = [&](int k) -> uint32_t {
+    if (hi_contig) return (uint32_t)k << hi_shift;
+    uint32_t g = 0;
+#pragma unroll
+    for (int b = 0; b < LCH; ++b)
+      if ((k >> b) & 1) g |= 1u << P.tile_bit[CB + LT + b];
+    return g;
+  };
 
   uint32_t tile = blockIdx.x;
   if (tile < P.n_tiles) {
-    const uint32_t base = tile_base_of<R, M, LR, LT>(tile, P) | g_t;
-    const uint32_t sb = smem_u32(bufs);
+    const uint32_t gb = tile_base_of<M>(tile, P) | g_t;
+    const uint32_t sb = smem_u32(bufs) + 16u * (uint32_t)tid;
 #pragma unroll
-    for (int k = 0; k < LPT; ++k) {
-      uint32_t g = base, s = s_t;
-#pragma unroll
-      for (int b = 0; b < LHI; ++b)
-        if ((k >> b) & 1) { g |= 1u << P.tile_bit[LT + b]; s ^= P.swz_tile[LT + b]; }
-      cp_async<CPB>(sb + s * (uint32_t)sizeof(T), src + g);
-    }
+    for (int k = 0; k < CPT; ++k) cp_async<16>(sb + 16u * (uint32_t)(k * NT), src + (gb | g_k(k)));
   }
   cp_async_commit();
   if (QFT && P.need_tw) __syncthreads();
@@ -241,52 +280,56 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
     T* cur = bufs + (it & 1) * E;
     const uint32_t next = tile + gridDim.x;
     if (next < P.n_tiles) {
-      const uint32_t nbase = tile_base_of<R, M, LR, LT>(next, P) | g_t;
-      const uint32_t sb = smem_u32(bufs + ((it + 1) & 1) * E);
+      const uint32_t gb = tile_base_of<M>(next, P) | g_t;
+      const uint32_t sb = smem_u32(bufs + ((it + 1) & 1) * E) + 16u * (uint32_t)tid;
 #pragma unroll
-      for (int k = 0; k < LPT; ++k) {
-        uint32_t g = nbase, s = s_t;
-#pragma unroll
-        for (int b = 0; b < LHI; ++b)
-          if ((k >> b) & 1) { g |= 1u << P.tile_bit[LT + b]; s ^= P.swz_tile[LT + b]; }
-        cp_async<CPB>(sb + s * (uint32_t)sizeof(T), src + g);
-      }
+      for (int k = 0; k < CPT; ++k) cp_async<16>(sb + 16u * (uint32_t)(k * NT), src + (gb | g_k(k)));
     }
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
-    const uint32_t base = tile_base_of<R, M, LR, LT>(tile, P);
+    const uint32_t base = tile_base_of<M>(tile, P);
     for (int ph = 0; ph < P.n_phases; ++ph) {
-      const PhaseDesc& D = P.ph[ph];
-      const int o0 = P.ph_op[ph], o1 = P.ph_op[ph + 1];
+      const PhaseDesc& D = phs[ph];
       uint32_t greg[LR], sreg[LR];
 #pragma unroll
-      for (int k = 0; k < LR; ++k) { greg[k] = D.g_reg[k]; sreg[k] = D.swz_reg[k]; }
+      for (int k = 0; k < LR; ++k) { greg[k] = D.g_reg[k]; sreg[k] = D.s_reg[k]; }
 #pragma unroll
       for (int g = 0; g < GPT; ++g) {
         const uint32_t q = (uint32_t)tid + (uint32_t)g * NT;
         uint32_t sq = 0, gq = base;
 #pragma unroll
         for (int j = 0; j < M - LR; ++j)
-          if ((q >> j) & 1) { sq ^= D.swz_grp[j]; gq |= D.g_grp[j]; }
+          if ((q >> j) & 1) { sq |= D.s_grp[j]; gq |= D.g_grp[j]; }
 #pragma unroll
-        for (int r = 0; r < NR; ++r) a[r] = cur[sq ^ xsel<LR>(r, sreg)];
-        for (int o = o0; o < o1; ++o) apply_op<R, LR, QFT>(a, P.ops[o], gq, greg, tw);
+        for (int r = 0; r < NR; ++r) a[r] = cur[sq + osel<LR>(r, sreg)];
+        if constexpr (QFT) {
+          for (int o = P.ph_op[ph]; o < P.ph_op[ph + 1]; ++o) apply_qft_op<R, LR>(a, P.ops[o], gq, greg, tw);
+        } else {
+          if (D.any_ctl) apply_u2_phase<R, LR, true>(a, D, gq, greg);
+          else apply_u2_phase<R, LR, false>(a, D, gq, greg);
+        }
 #pragma unroll
-        for (int r = 0; r < NR; ++r) cur[sq ^ xsel<LR>(r, sreg)] = a[r];
+        for (int r = 0; r < NR; ++r) cur[sq + osel<LR>(r, sreg)] = a[r];
       }
       __syncthreads();
     }
     const uint32_t gb = base | g_t;
+    const float4* c4 = reinterpret_cast<const float4*>(cur) + tid;
 #pragma unroll
-    for (int k = 0; k < LPT; ++k) {
-      uint32_t g = gb, s = s_t;
-#pragma unroll
-      for (int b = 0; b < LHI; ++b)
-        if ((k >> b) & 1) { g |= 1u << P.tile_bit[LT + b]; s ^= P.swz_tile[LT + b]; }
-      T v = cur[s];
-      if (QFT) v = cscale(v, (R)P.scale);
-      dst[g] = v;
+    for (int k = 0; k < CPT; ++k) {
+      float4 v = c4[k * NT];
+      if (QFT) {
+        if constexpr (sizeof(R) == 4) {
+          const float sc = (float)P.scale;
+          v.x *= sc; v.y *= sc; v.z *= sc; v.w *= sc;
+        } else {
+          double2 d = *reinterpret_cast<double2*>(&v);
+          d.x *= P.scale; d.y *= P.scale;
+          v = *reinterpret_cast<float4*>(&d);
+        }
+      }
+      *reinterpret_cast<float4*>(dst + (gb | g_k(k))) = v;
     }
     __syncthreads();
   }
@@ -310,9 +353,16 @@ static int env_int(const char* name, int dflt, int lo, int hi) {
   return std::min(hi, std::max(lo, x));
 }
 
-static int reg_bits(int dtype, int m) { return std::min(m, dtype == MQ_C64 ? 5 : 4); }
-static int tile_max(int dtype) { return dtype == MQ_C64 ? env_int("MQ_TILE_MAX", 12, 6, 12) : 11; }
-static int passengers() { return env_int("MQ_TILE_PASSENGERS", 3, 0, 5); }
+static int reg_bits(int dtype, int m) {
+  const int lr = dtype == MQ_C64 ? env_int("MQ_TILE_LR", 4, 4, 5) : 4;
+  return std::min(m, lr);
+}
+static int tile_max(int dtype) {
+  if (dtype != MQ_C64) return 11;
+  const int lim = reg_bits(MQ_C64, 13) == 4 ? 13 : 12;
+  return env_int("MQ_TILE_MAX", 12, 6, lim);
+}
+static int passengers() { return env_int("MQ_TILE_PASSENGERS", 4, 0, 5); }
 static int min_tile() { return env_int("MQ_TILE_MIN", 10, 1, 12); }
 
 // Register phases: targets (tile-local) chunked in the given order into
@@ -343,63 +393,6 @@ static void make_phases(int m, int lr, const std::vector<int>& order, Sweep& sw,
   }
 }
 
-// Swizzle: the shared-memory offset of tile bit b is (1 << b) ^ S(b) with
-// S(b) confined to the low `lb` bits (S(b) = 0 for b < lb).  For every phase,
-// the lowest lb group bits (the lanes of one shared-memory wavefront) must
-// map to independent low-bit patterns.  Small backtracking search; S = 0
-// (correct, possibly conflicted) if none is found.
-static bool independent(const std::vector<uint32_t>& v) {
-  uint32_t basis[8] = {0};
-  for (uint32_t x : v) {
-    for (int p = 7; p >= 0; --p) {
-      if (!((x >> p) & 1u)) continue;
-      if (basis[p]) x ^= basis[p];
-      else { basis[p] = x; break; }
-    }
-    if (!x) return false;
-  }
-  return true;
-}
-
-static std::vector<uint32_t> solve_swizzle(int m, int lb, const std::vector<std::vector<int>>& phases) {
-  std::vector<std::vector<int>> lanes;
-  for (auto& regs : phases) {
-    std::vector<int> grp;
-    for (int b = 0; b < m && (int)grp.size() < lb; ++b)
-      if (std::find(regs.begin(), regs.end(), b) == regs.end()) grp.push_back(b);
-    lanes.push_back(grp);
-  }
-  std::vector<uint32_t> S(m, 0);
-  const uint32_t full = (1u << lb) - 1u;
-  auto img = [&](int b) -> uint32_t { return b < lb ? (1u << b) : S[b]; };
-  auto ok_upto = [&](int upto) {
-    for (auto& grp : lanes) {
-      if ((int)grp.size() < lb) continue;
-      bool determined = true;
-      for (int b : grp)
-        if (b >= lb && b > upto) determined = false;
-      if (!determined) continue;
-      std::vector<uint32_t> v;
-      for (int b : grp) v.push_back(img(b));
-      if (!independent(v)) return false;
-    }
-    return true;
-  };
-  int nodes = 0;
-  std::function<bool(int)> rec = [&](int b) -> bool {
-    if (b >= m) return true;
-    if (++nodes > 100000) return false;
-    for (uint32_t c = 1; c <= full; ++c) {
-      S[b] = c;
-      if (ok_upto(b) && rec(b + 1)) return true;
-    }
-    S[b] = 0;
-    return false;
-  };
-  if (m <= lb || rec(lb)) return S;
-  return std::vector<uint32_t>(m, 0);
-}
-
 template <typename R, int M, int LR, int LT, bool QFT>
 static int launch_tile_t(mq_state* h, const TileParams& P, size_t smem, bool out_of_place) {
   auto kern = k_tile<R, M, LR, LT, QFT>;
@@ -422,37 +415,48 @@ static int launch_tile_t(mq_state* h, const TileParams& P, size_t smem, bool out
   return MQ_OK;
 }
 
-template <typename R, bool QFT>
-static int dispatch_tile(mq_state* h, const TileParams& P, size_t smem) {
-  constexpr bool F = sizeof(R) == 4;
-  constexpr int LRMAX = F ? 5 : 4;
+template <typename R, bool QFT, int LR>
+static int dispatch_tile_lr(mq_state* h, const TileParams& P, size_t smem) {
   switch (P.m) {
 #define MQ_TILE_CASE(MM)                                                        \
     case MM: {                                                                  \
-      constexpr int LR = (MM) < LRMAX ? (MM) : LRMAX;                           \
-      constexpr int LT = ((MM) - LR) < 7 ? ((MM) - LR) : 7;                     \
-      return launch_tile_t<R, MM, LR, LT, QFT>(h, P, smem, false);                  \
+      constexpr int L = (MM) < LR ? (MM) : LR;                                  \
+      constexpr int LT = ((MM) - L) < 8 ? ((MM) - L) : 8;                       \
+      return launch_tile_t<R, MM, L, LT, QFT>(h, P, smem, false);              \
     }
     MQ_TILE_CASE(1) MQ_TILE_CASE(2) MQ_TILE_CASE(3) MQ_TILE_CASE(4) MQ_TILE_CASE(5) MQ_TILE_CASE(6)
     MQ_TILE_CASE(7) MQ_TILE_CASE(8) MQ_TILE_CASE(9) MQ_TILE_CASE(10) MQ_TILE_CASE(11)
 #undef MQ_TILE_CASE
     case 12:
-      if constexpr (F) return launch_tile_t<R, 12, 5, 7, QFT>(h, P, smem, false);
+      if constexpr (sizeof(R) == 4) {
+        constexpr int LT = LR == 5 ? 7 : 8;
+        return launch_tile_t<R, 12, LR, LT, QFT>(h, P, smem, false);
+      }
+      break;
+    case 13:
+      if constexpr (sizeof(R) == 4 && LR == 4) return launch_tile_t<R, 13, 4, 9, QFT>(h, P, smem, false);
       break;
     default: break;
   }
   return fail(MQ_EUNSUPPORTED, "tile size not instantiated");
 }
 
+template <typename R, bool QFT>
+static int dispatch_tile(mq_state* h, const TileParams& P, size_t smem) {
+  if constexpr (sizeof(R) == 4) {
+    if (reg_bits(MQ_C64, 12) == 4) return dispatch_tile_lr<R, QFT, 4>(h, P, smem);
+    return dispatch_tile_lr<R, QFT, 5>(h, P, smem);
+  }
+  return dispatch_tile_lr<R, QFT, 4>(h, P, smem);
+}
+
 static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, const std::vector<int>& op_rk) {
   const int m = (int)sw.tile_bits.size();
   const int lr = reg_bits(h->dtype, m);
   if (m < 1 || m > tile_max(h->dtype) || m > h->n) return fail(MQ_EINVAL, "bad tile size");
+  if (sw.tile_bits[0] != 0) return fail(MQ_EINVAL, "tile must contain index bit 0");
   if ((int)sw.ops.size() > kMaxOps || (int)sw.phases.size() > kMaxPhases) return fail(MQ_EINVAL, "tile plan too large");
-  const int lb = std::min(m, h->dtype == MQ_C64 ? 4 : 3);  // 2^lb lanes per shared-memory wavefront
-  std::vector<uint32_t> S = env_int("MQ_TILE_SWIZZLE", 1, 0, 1) ? solve_swizzle(m, lb, sw.phases)
-                                                                 : std::vector<uint32_t>(m, 0);
-  auto swz_of = [&](int b) -> uint16_t { return (uint16_t)((1u << b) ^ S[b]); };
+  const bool qft = !sw.ops.empty() && (sw.ops[0].kind == OP_QFT_FWD || sw.ops[0].kind == OP_QFT_INV);
   TileParams P;
   std::memset(&P, 0, sizeof(P));
   P.n_tiles = (uint32_t)(uint64_t(1) << (h->n - m));
@@ -460,47 +464,65 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
   P.m = (uint8_t)m;
   P.n_phases = (uint8_t)sw.phases.size();
   P.n_ops = (uint8_t)sw.ops.size();
-  for (int k = 0; k < m; ++k) {
-    P.tile_bit[k] = (uint8_t)sw.tile_bits[k];
-    P.swz_tile[k] = swz_of(k);
+  for (int k = 0; k < m; ++k) P.tile_bit[k] = (uint8_t)sw.tile_bits[k];
+  // chunk-index bits above the thread bits: contiguous global bits?
+  {
+    const int cb = h->dtype == MQ_C64 ? 1 : 0;
+    const int lt = (m == 12 && lr == 5) ? 7 : (m == 13 ? 9 : std::min(8, m - lr));
+    const int first = cb + lt;
+    bool contig = true;
+    for (int b = first + 1; b < m; ++b)
+      if (sw.tile_bits[b] != sw.tile_bits[b - 1] + 1) contig = false;
+    P.hi_contig = (first < m && contig) ? 1 : 0;
+    P.hi_shift = (uint8_t)(first < m ? sw.tile_bits[first] : 0);
   }
   for (size_t p = 0; p < sw.phases.size(); ++p) {
     const auto& regs = sw.phases[p];
     PhaseDesc& D = P.ph[p];
     for (int k = 0; k < lr; ++k) {
-      D.swz_reg[k] = swz_of(regs[k]);
+      D.s_reg[k] = 1u << regs[k];
       D.g_reg[k] = 1u << sw.tile_bits[regs[k]];
     }
     int j = 0;
     for (int b = 0; b < m; ++b) {
       if (std::find(regs.begin(), regs.end(), b) != regs.end()) continue;
-      D.swz_grp[j] = swz_of(b);
+      D.s_grp[j] = 1u << b;
       D.g_grp[j] = 1u << sw.tile_bits[b];
       ++j;
     }
   }
-  // ops grouped by phase, original order kept inside each phase
-  {
+  if (qft) {
     int w = 0;
     for (size_t p = 0; p < sw.phases.size(); ++p) {
       P.ph_op[p] = (uint8_t)w;
       for (size_t o = 0; o < sw.ops.size(); ++o) {
         if (op_phase[o] != (int)p) continue;
         P.ops[w] = sw.ops[o];
-        for (int j = 0; j < 8; ++j) P.ops[w].uf[j] = (float)sw.ops[o].u[j];
         P.ops[w].phase = (uint8_t)p;
         P.ops[w].rk = (uint8_t)op_rk[o];
         ++w;
       }
     }
     P.ph_op[sw.phases.size()] = (uint8_t)w;
+  } else {
+    for (size_t o = 0; o < sw.ops.size(); ++o) {
+      PhaseDesc& D = P.ph[op_phase[o]];
+      const int k = op_rk[o];
+      if (D.active & (1u << k)) return fail(MQ_EINVAL, "two gates on one register slot");
+      D.active |= (uint8_t)(1u << k);
+      D.cmask[k] = sw.ops[o].kind == OP_CU2 ? sw.ops[o].cmask : 0u;
+      if (D.cmask[k]) D.any_ctl = 1;
+      for (int j = 0; j < 8; ++j) {
+        D.ud[k][j] = sw.ops[o].u[j];
+        D.uf[k][j] = (float)sw.ops[o].u[j];
+      }
+    }
   }
-  P.need_tw = (sw.need_tw && h->dtype == MQ_C64) ? 1 : 0;
+  P.need_tw = (qft && sw.need_tw && h->dtype == MQ_C64) ? 1 : 0;
   P.has_scale = sw.has_scale ? 1 : 0;
   P.scale = sw.has_scale ? sw.scale : 1.0;
-  size_t smem = 2 * (h->amp_bytes() << m);
+  size_t smem = 2 * (h->amp_bytes() << m) + sizeof(PhaseDesc) * kMaxPhases;
   if (P.need_tw) smem += 3072 * sizeof(float2);
-  const bool qft = !sw.ops.empty() && (sw.ops[0].kind == OP_QFT_FWD || sw.ops[0].kind == OP_QFT_INV);
   if (h->dtype == MQ_C64) return qft ? dispatch_tile<float, true>(h, P, smem) : dispatch_tile<float, false>(h, P, smem);
   return qft ? dispatch_tile<double, true>(h, P, smem) : dispatch_tile<double, false>(h, P, smem);
 }
@@ -516,7 +538,7 @@ static int tile_local(const std::vector<int>& bits, int gbit) {
 static std::vector<int> tile_for(int n, const std::vector<int>& targets, int pas, int tmax) {
   std::vector<int> bits = targets;
   const int lowest = *std::min_element(targets.begin(), targets.end());
-  for (int b = 0; b < std::min(pas, lowest); ++b) bits.push_back(b);
+  for (int b = 0; b < std::min(std::max(pas, 1), lowest); ++b) bits.push_back(b);
   std::sort(bits.begin(), bits.end());
   bits.erase(std::unique(bits.begin(), bits.end()), bits.end());
   const int want = std::min({n, min_tile(), tmax});
