@@ -133,6 +133,24 @@ int mq_sample(mq_state* h, const int32_t* wires, int k, uint64_t seed,
  * out[2w+1] = im (integrations/_common.py:384-427). */
 int mq_expval_pauli(mq_state* h, int n_words, const uint64_t* xmask,
                     const uint64_t* zmask, const int32_t* ny, double* out);
+/* mq_expval_pauli without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc or cudaFree
+ * in the middle of their work -- a serving loop that admits requests by
+ * state footprint alone and must not let a measurement grow device memory,
+ * a host whose own pool already owns the free HBM, or one that cannot let
+ * cudaFree's device-wide wait stall its other streams.
+ * Same arguments and the same result bits as mq_expval_pauli.  Its scratch
+ * is a fixed 131,200-byte device array inside the library, held by every
+ * GPU that loads it until the process exits; it holds the partial sums of
+ * up to 1024 blocks, enough for GPUs of up to 256 SMs, and larger GPUs get
+ * MQ_EUNSUPPORTED.  The first call on each device looks up the array's
+ * device address; make that first call before any stream capture.  All
+ * calls on one device share the array: calls that overlap on the GPU (other
+ * handles, other streams) race and must be serialised by the caller.  Each
+ * call writes every scratch slot it reads, so nothing needs clearing
+ * between calls. */
+int mq_expval_pauli_static(mq_state* h, int n_words, const uint64_t* xmask,
+                           const uint64_t* zmask, const int32_t* ny, double* out);
 
 #ifdef __cplusplus
 }

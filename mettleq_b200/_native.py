@@ -53,6 +53,7 @@ SIGNATURES = {
     "mq_probabilities": (_I, [_P, _P, _I, _I, _P]),
     "mq_sample": (_I, [_P, _P, _I, _U64, _U64, _I64, _P]),
     "mq_expval_pauli": (_I, [_P, _I, _P, _P, _P, _P]),
+    "mq_expval_pauli_static": (_I, [_P, _I, _P, _P, _P, _P]),
 }
 
 

@@ -420,4 +420,17 @@ int mq_expval_pauli(mq_state* h, int n_words, const uint64_t* xmask, const uint6
   MQ_TRY_END
 }
 
+// Allocation-free variant of mq_expval_pauli; see include/mq.h.
+int mq_expval_pauli_static(mq_state* h, int n_words, const uint64_t* xmask, const uint64_t* zmask,
+                           const int32_t* ny, double* out) {
+  MQ_TRY_BEGIN
+  MQ_CHECK_HANDLE(h);
+  if (n_words < 0) return fail(MQ_EINVAL, "negative word count");
+  if (n_words == 0) return MQ_OK;
+  if (!xmask || !zmask || !out) return fail(MQ_EINVAL, "null Pauli arrays");
+  DeviceGuard g(h->device);
+  return run_expval_pauli_static(h, n_words, xmask, zmask, ny, out);
+  MQ_TRY_END
+}
+
 }  // extern "C"

@@ -125,6 +125,9 @@ int run_sample(mq_state* h, const int32_t* wires, int k, uint64_t seed, uint64_t
                int64_t shots, int64_t* out);
 int run_expval_pauli(mq_state* h, int n_words, const uint64_t* xmask, const uint64_t* zmask,
                      const int32_t* ny, double* out);
+// Same values through a fixed file-scope device array: allocates nothing.
+int run_expval_pauli_static(mq_state* h, int n_words, const uint64_t* xmask, const uint64_t* zmask,
+                            const int32_t* ny, double* out);
 
 // GF(2) helpers (host)
 bool gf2_invert(int n, const uint32_t* cols, uint32_t* inv_cols);

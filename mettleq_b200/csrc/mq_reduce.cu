@@ -16,6 +16,8 @@
 // offsets and a sequential running sum inside the chosen block.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "mq_internal.cuh"
@@ -463,6 +465,113 @@ int run_expval_pauli(mq_state* h, int n_words, const uint64_t* xmask, const uint
       out[2 * w] = fr;
       out[2 * w + 1] = fi;
     }
+  }
+  return MQ_OK;
+}
+
+// ================================================ allocation-free expectations
+// mq_expval_pauli_static computes the same values as mq_expval_pauli, but
+// never allocates device memory.  mq_expval_pauli grows the handle's scratch
+// buffer with cudaMalloc (and cudaFree) the first time it needs room for
+// its per-block partial sums; cudaFree waits for the whole device.  Callers
+// that run under a fixed device-memory budget (a serving loop that admits
+// requests by their state footprint alone, or a host whose memory pool owns
+// all free HBM) or that cannot stall other streams with that device-wide
+// wait use this entry point instead.
+//
+// Its scratch is a file-scope device array of a fixed size: every GPU that
+// loads the library holds these 131,200 bytes until the process exits.  The
+// host reaches the array through the address that cudaGetSymbolAddress
+// returns for the current device (the array's name in host code is only a
+// host-side stand-in); the address is looked up once per device, on the
+// first call made on that device.
+constexpr uint32_t kStaticBlocks = 1024;  // partial-sum blocks the array holds
+static __device__ __align__(256) double2 g_pauli_static[kStaticBlocks * kWords + kWords];
+
+constexpr int kStaticMaxDevices = 64;
+static std::mutex g_static_mu;
+static void* g_static_addr[kStaticMaxDevices] = {};
+
+// Device address of g_pauli_static on `device`, which must be current.
+static int pauli_static_scratch(int device, double2** out) {
+  if (device < 0 || device >= kStaticMaxDevices) return fail(MQ_EUNSUPPORTED, "device ordinal beyond 63");
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_addr[device]) {
+    void* p = nullptr;
+    MQ_CUDA(cudaGetSymbolAddress(&p, g_pauli_static));
+    g_static_addr[device] = p;
+  }
+  *out = reinterpret_cast<double2*>(g_static_addr[device]);
+  return MQ_OK;
+}
+
+// res[w] = sum over blocks b of partials[b][w], in increasing b: the order
+// and rounding of the host loop in run_expval_pauli, so both entry points
+// return the same bits.
+__global__ void k_pauli_finish(const double2* __restrict__ partials, uint32_t nblocks, int nw,
+                               double2* __restrict__ res) {
+  const int w = threadIdx.x;
+  if (w >= nw) return;
+  double re = 0.0, im = 0.0;
+  for (uint32_t b = 0; b < nblocks; ++b) {
+    re = __dadd_rn(re, partials[b * kWords + w].x);
+    im = __dadd_rn(im, partials[b * kWords + w].y);
+  }
+  res[w] = make_double2(re, im);
+}
+
+int run_expval_pauli_static(mq_state* h, int n_words, const uint64_t* xmask, const uint64_t* zmask,
+                            const int32_t* ny, double* out) {
+  const uint64_t lim = h->dim() - 1;
+  for (int w = 0; w < n_words; ++w)
+    if ((xmask[w] & ~lim) || (zmask[w] & ~lim)) return fail(MQ_EINVAL, "Pauli mask outside the register");
+  // same grid as run_expval_pauli: the partial sums, and so the result bits,
+  // depend on it
+  const uint32_t grid = (uint32_t)h->num_sms * 4;
+  if (grid > kStaticBlocks)
+    return fail(MQ_EUNSUPPORTED, "mq_expval_pauli_static: this GPU needs " + std::to_string(grid) +
+                                     " partial-sum blocks; the static scratch holds 1024 (GPUs of up to 256 SMs)");
+  double2* partials = nullptr;
+  int rc = pauli_static_scratch(h->device, &partials);
+  if (rc) return rc;
+  double2* res = partials + (size_t)kStaticBlocks * kWords;
+  // Every slot read below is written earlier in the same call (k_pauli writes
+  // all kWords slots of each of its blocks, k_pauli_finish all nw results it
+  // returns), so whatever an earlier call left in the array is never read
+  // and nothing has to be cleared.
+  int w0 = 0;
+  while (w0 < n_words) {
+    // consecutive words with one X/Y mask share a pass over the state
+    int cnt = 1;
+    while (w0 + cnt < n_words && cnt < kWords && xmask[w0 + cnt] == xmask[w0]) ++cnt;
+    PauliParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.dim = (uint32_t)h->dim();
+    P.x = (uint32_t)xmask[w0];
+    P.nw = cnt;
+    for (int i = 0; i < cnt; ++i) P.z[i] = (uint32_t)zmask[w0 + i];
+    if (h->dtype == MQ_C64) k_pauli<float><<<grid, 256, 0, h->stream>>>((const float2*)h->cur_buf(), P, partials);
+    else k_pauli<double><<<grid, 256, 0, h->stream>>>((const double2*)h->cur_buf(), P, partials);
+    MQ_LAUNCHED("k_pauli");
+    k_pauli_finish<<<1, 32, 0, h->stream>>>(partials, grid, cnt, res);
+    MQ_LAUNCHED("k_pauli_finish");
+    h->launches += 2;
+    h->sweeps += 1;
+    double2 host[kWords];
+    MQ_CUDA(cudaMemcpyAsync(host, res, (size_t)cnt * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    MQ_CUDA(cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < cnt; ++i) {
+      const int w = w0 + i;
+      const double re = host[i].x, im = host[i].y;
+      const int r = ((ny ? ny[w] : 0) % 4 + 4) % 4;  // multiply by i^ny
+      double fr = re, fi = im;
+      if (r == 1) { fr = -im; fi = re; }
+      else if (r == 2) { fr = -re; fi = -im; }
+      else if (r == 3) { fr = im; fi = -re; }
+      out[2 * w] = fr;
+      out[2 * w + 1] = fi;
+    }
+    w0 += cnt;
   }
   return MQ_OK;
 }
