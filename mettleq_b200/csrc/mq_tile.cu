@@ -16,8 +16,9 @@
 //     thread loads 2^LR amplitudes that differ in LR tile bits into
 //     registers, applies the gates of those bits, and writes them back;
 //   * global memory moves in 16-byte chunks, loaded with cp.async and stored
-//     with vector stores, in a tile-local = shared-memory index layout, so
-//     all load/store offsets are compile-time immediates;
+//     with vector stores; shared memory holds the tile in a chunk-swizzled
+//     layout (see k_tile) so register phases over the lowest bits stay free
+//     of bank conflicts;
 //   * the finished tile is written back with coalesced stores.
 //
 // QFT stages (sim.py:522-563, no final swaps): stage j on index bit s is a
@@ -104,7 +105,7 @@ __device__ __forceinline__ uint32_t osel(int r, const uint32_t* g) {
   uint32_t o = 0;
 #pragma unroll
   for (int k = 0; k < LR; ++k)
-    if (r & (1 << k)) o |= g[k];
+    if (r & (1 << k)) o ^= g[k];
   return o;
 }
 
@@ -209,12 +210,19 @@ __device__ __forceinline__ uint32_t tile_base_of(uint32_t tile, const TileParams
   return (uint32_t)x;
 }
 
-// Tile of 2^M amplitudes in an identity shared-memory layout (tile-local
-// index = shared-memory index), 2^LT threads, 2^LR amplitudes per register
+// Tile of 2^M amplitudes, 2^LT threads, 2^LR amplitudes per register
 // group.  Global traffic moves in 16-byte chunks (two complex64 or one
 // complex128 amplitude): chunk c covers tile-local element c << CB.
+//
+// Shared-memory layout: chunk c sits at chunk slot swz(c) = c ^ ((c >> 3) & 7),
+// i.e. the chunk's position inside its 128-byte row is XORed with the next
+// three chunk-index bits.  swz is linear over GF(2), so the slot of an
+// amplitude is the XOR of the slots of its index bits; the host stores those
+// per-bit slots (PhaseDesc s_reg / s_grp) and the kernel combines them with
+// XOR.  Without it, a register phase over tile bits 0-3 (the low sweep) has
+// the 16 threads of a half-warp 128 bytes apart, all in one bank pair.
 template <typename R, int M, int LR, int LT, bool QFT>
-__global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? 2 : (LT >= 7 ? 3 : 1))))
+__global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? 3 : (LT >= 7 ? (sizeof(R) == 4 && LR == 4 ? 6 : 3) : (LT >= 6 && sizeof(R) == 4 ? 8 : 1)))))
 k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
   using T = V2<R>;
   constexpr int NT = 1 << LT;
@@ -255,6 +263,13 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
 #pragma unroll
   for (int b = 0; b < LT; ++b)
     if ((tid >> b) & 1) g_t |= 1u << P.tile_bit[CB + b];
+  // swz(tid + k*NT) = swz(tid) ^ swz(k*NT) (tid < NT, swz linear); the
+  // second term is a compile-time value once the k loops are unrolled
+  const uint32_t s_t = (uint32_t)tid ^ (((uint32_t)tid >> 3) & 7u);
+  auto slot = [&](int k) -> uint32_t {
+    const uint32_t kk = (uint32_t)(k * NT);
+    return s_t ^ (kk ^ ((kk >> 3) & 7u));
+  };
   const bool hi_contig = P.hi_contig;
   const int hi_shift = P.hi_shift;
   auto g_k = [&](int k) -> uint32_t {
@@ -269,9 +284,9 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
   uint32_t tile = blockIdx.x;
   if (tile < P.n_tiles) {
     const uint32_t gb = tile_base_of<M>(tile, P) | g_t;
-    const uint32_t sb = smem_u32(bufs) + 16u * (uint32_t)tid;
+    const uint32_t sb = smem_u32(bufs);
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) cp_async<16>(sb + 16u * (uint32_t)(k * NT), src + (gb | g_k(k)));
+    for (int k = 0; k < CPT; ++k) cp_async<16>(sb + 16u * slot(k), src + (gb | g_k(k)));
   }
   cp_async_commit();
   if (QFT && P.need_tw) __syncthreads();
@@ -281,9 +296,9 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
     const uint32_t next = tile + gridDim.x;
     if (next < P.n_tiles) {
       const uint32_t gb = tile_base_of<M>(next, P) | g_t;
-      const uint32_t sb = smem_u32(bufs + ((it + 1) & 1) * E) + 16u * (uint32_t)tid;
+      const uint32_t sb = smem_u32(bufs + ((it + 1) & 1) * E);
 #pragma unroll
-      for (int k = 0; k < CPT; ++k) cp_async<16>(sb + 16u * (uint32_t)(k * NT), src + (gb | g_k(k)));
+      for (int k = 0; k < CPT; ++k) cp_async<16>(sb + 16u * slot(k), src + (gb | g_k(k)));
     }
     cp_async_commit();
     cp_async_wait<1>();
@@ -300,25 +315,45 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
         uint32_t sq = 0, gq = base;
 #pragma unroll
         for (int j = 0; j < M - LR; ++j)
-          if ((q >> j) & 1) { sq |= D.s_grp[j]; gq |= D.g_grp[j]; }
+          if ((q >> j) & 1) { sq ^= D.s_grp[j]; gq |= D.g_grp[j]; }
+        // complex64 with tile bit 0 in register slot 0: amplitudes r, r+1 share
+        // one 16-byte chunk, read as one vector (a quarter-warp then covers
+        // all eight chunk slots of a row)
+        const bool pair = sizeof(R) == 4 && sreg[0] == 1u;
+        if (pair) {
 #pragma unroll
-        for (int r = 0; r < NR; ++r) a[r] = cur[sq + osel<LR>(r, sreg)];
+          for (int r = 0; r < NR; r += 2) {
+            const float4 v = *reinterpret_cast<const float4*>(cur + (sq ^ osel<LR>(r, sreg)));
+            a[r] = mk<R>((R)v.x, (R)v.y);
+            a[r + 1] = mk<R>((R)v.z, (R)v.w);
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < NR; ++r) a[r] = cur[sq ^ osel<LR>(r, sreg)];
+        }
         if constexpr (QFT) {
           for (int o = P.ph_op[ph]; o < P.ph_op[ph + 1]; ++o) apply_qft_op<R, LR>(a, P.ops[o], gq, greg, tw);
         } else {
           if (D.any_ctl) apply_u2_phase<R, LR, true>(a, D, gq, greg);
           else apply_u2_phase<R, LR, false>(a, D, gq, greg);
         }
+        if (pair) {
 #pragma unroll
-        for (int r = 0; r < NR; ++r) cur[sq + osel<LR>(r, sreg)] = a[r];
+          for (int r = 0; r < NR; r += 2)
+            *reinterpret_cast<float4*>(cur + (sq ^ osel<LR>(r, sreg))) =
+                make_float4((float)a[r].x, (float)a[r].y, (float)a[r + 1].x, (float)a[r + 1].y);
+        } else {
+#pragma unroll
+          for (int r = 0; r < NR; ++r) cur[sq ^ osel<LR>(r, sreg)] = a[r];
+        }
       }
       __syncthreads();
     }
     const uint32_t gb = base | g_t;
-    const float4* c4 = reinterpret_cast<const float4*>(cur) + tid;
+    const float4* c4 = reinterpret_cast<const float4*>(cur);
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-      float4 v = c4[k * NT];
+      float4 v = c4[slot(k)];
       if (QFT) {
         if constexpr (sizeof(R) == 4) {
           const float sc = (float)P.scale;
@@ -366,24 +401,23 @@ static int passengers() { return env_int("MQ_TILE_PASSENGERS", 4, 0, 5); }
 static int min_tile() { return env_int("MQ_TILE_MIN", 10, 1, 12); }
 
 // Register phases: targets (tile-local) chunked in the given order into
-// groups of LR; the last group is padded with non-target bits.  Records the
-// phase index and register slot of every target.
+// groups of LR; the last group is padded with the highest tile bits it does
+// not hold (targets of other phases included: a slot without a gate is left
+// alone), which keeps tile bits 0-3 as thread bits and shared-memory access
+// free of bank conflicts.  Records the phase index and register slot of
+// every target.
 static void make_phases(int m, int lr, const std::vector<int>& order, Sweep& sw, std::vector<int>& op_phase,
                         std::vector<int>& op_rk) {
   sw.phases.clear();
   op_phase.assign(order.size(), 0);
   op_rk.assign(order.size(), 0);
-  std::vector<bool> is_target(m, false);
-  for (int t : order) is_target[t] = true;
   for (size_t i = 0; i < order.size(); i += lr) {
     std::vector<int> regs;
     for (size_t j = i; j < std::min(order.size(), i + lr); ++j) {
       op_phase[j] = (int)sw.phases.size();
       regs.push_back(order[j]);
     }
-    for (int b = 0; (int)regs.size() < lr && b < m; ++b)
-      if (std::find(regs.begin(), regs.end(), b) == regs.end() && !is_target[b]) regs.push_back(b);
-    for (int b = 0; (int)regs.size() < lr && b < m; ++b)
+    for (int b = m - 1; (int)regs.size() < lr && b >= 0; --b)
       if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
     std::vector<int> sorted = regs;
     std::sort(sorted.begin(), sorted.end());
@@ -476,17 +510,21 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
     P.hi_contig = (first < m && contig) ? 1 : 0;
     P.hi_shift = (uint8_t)(first < m ? sw.tile_bits[first] : 0);
   }
+  // shared-memory slot of tile-local amplitude index i (the chunk swizzle
+  // of k_tile applied at amplitude granularity)
+  const bool c64 = h->dtype == MQ_C64;
+  auto phys = [c64](uint32_t i) -> uint32_t { return c64 ? (i ^ ((i >> 3) & 0xEu)) : (i ^ ((i >> 3) & 7u)); };
   for (size_t p = 0; p < sw.phases.size(); ++p) {
     const auto& regs = sw.phases[p];
     PhaseDesc& D = P.ph[p];
     for (int k = 0; k < lr; ++k) {
-      D.s_reg[k] = 1u << regs[k];
+      D.s_reg[k] = phys(1u << regs[k]);
       D.g_reg[k] = 1u << sw.tile_bits[regs[k]];
     }
     int j = 0;
     for (int b = 0; b < m; ++b) {
       if (std::find(regs.begin(), regs.end(), b) != regs.end()) continue;
-      D.s_grp[j] = 1u << b;
+      D.s_grp[j] = phys(1u << b);
       D.g_grp[j] = 1u << sw.tile_bits[b];
       ++j;
     }
