@@ -105,6 +105,18 @@ int mq_apply_diag_terms(mq_state* h, int n_terms, const int32_t* kinds,
 int mq_apply_diag_layer(mq_state* h, int kind, int n_bonds, const int32_t* bonds,
                         const double* thetas);
 
+/* ---- fused layer (device.py:1089-1097 dispatch of one config-0 layer) ---- */
+/* U(2) on every qubit with active[q] != 0 (mats as in mq_apply_u2_layer;
+ * mats == NULL: none), then the diagonal terms (as in mq_apply_diag_terms;
+ * n_terms may be 0), then the GF(2) permutation of mq_apply_xor_affine
+ * (rows == NULL: none).  The result equals the three calls in that order;
+ * the diagonal and a permutation that keeps the low index bits among
+ * themselves (CNOT ladders) ride on the last U(2) sweep instead of taking
+ * sweeps of their own. */
+int mq_apply_layer(mq_state* h, const double* mats, const uint8_t* active,
+                   int n_terms, const int32_t* kinds, const int32_t* wires,
+                   const double* params, const uint64_t* rows, uint64_t c);
+
 /* ---- (c) QFT (shaders/qft.py:144-236, sim.py:522-563) -------------------- */
 /* Ordered wire list, first wire = most significant logical bit, no final
  * swaps; inverse != 0 applies iqft. */

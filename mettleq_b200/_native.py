@@ -50,6 +50,7 @@ SIGNATURES = {
     "mq_apply_qft": (_I, [_P, _P, _I, _I]),
     "mq_apply_qft_stages": (_I, [_P, _I, _I, _I, _I, _I]),
     "mq_apply_xor_affine": (_I, [_P, _P, _U64]),
+    "mq_apply_layer": (_I, [_P, _P, _P, _I, _P, _P, _P, _P, _U64]),
     "mq_probabilities": (_I, [_P, _P, _I, _I, _P]),
     "mq_sample": (_I, [_P, _P, _I, _U64, _U64, _I64, _P]),
     "mq_expval_pauli": (_I, [_P, _I, _P, _P, _P, _P]),

@@ -367,20 +367,44 @@ int mq_apply_qft(mq_state* h, const int32_t* wires, int k, int inverse) {
   MQ_TRY_END
 }
 
-int mq_apply_xor_affine(mq_state* h, const uint64_t* rows, uint64_t c) {
-  MQ_TRY_BEGIN
-  MQ_CHECK_HANDLE(h);
-  if (!rows) return fail(MQ_EINVAL, "null rows");
+// rows (inverse-map rows, qubit k = row k) -> columns A e_j of the source
+// map over index bits; validates the masks.
+static int rows_to_cols(const mq_state* h, const uint64_t* rows, uint64_t c, uint32_t* cols) {
   const int n = h->n;
   const uint64_t lim = h->dim() - 1;
   if (c & ~lim) return fail(MQ_EINVAL, "flip constant outside the register");
-  uint32_t cols[32];
   for (int j = 0; j < n; ++j) cols[j] = 0;
   for (int k = 0; k < n; ++k) {
     if (rows[k] & ~lim) return fail(MQ_EINVAL, "affine row outside the register");
     for (int j = 0; j < n; ++j)
       if ((rows[k] >> j) & 1u) cols[j] |= 1u << (n - 1 - k);
   }
+  return MQ_OK;
+}
+
+int mq_apply_layer(mq_state* h, const double* mats, const uint8_t* active, int n_terms, const int32_t* kinds,
+                   const int32_t* wires, const double* params, const uint64_t* rows, uint64_t c) {
+  MQ_TRY_BEGIN
+  MQ_CHECK_HANDLE(h);
+  if (n_terms < 0) return fail(MQ_EINVAL, "negative term count");
+  if (n_terms > 0 && (!kinds || !wires || !params)) return fail(MQ_EINVAL, "null term arrays");
+  uint32_t cols[32];
+  if (rows) {
+    int rc = rows_to_cols(h, rows, c, cols);
+    if (rc) return rc;
+  }
+  DeviceGuard g(h->device);
+  return launch_layer(h, mats, active, n_terms, kinds, wires, params, rows ? cols : nullptr, (uint32_t)c);
+  MQ_TRY_END
+}
+
+int mq_apply_xor_affine(mq_state* h, const uint64_t* rows, uint64_t c) {
+  MQ_TRY_BEGIN
+  MQ_CHECK_HANDLE(h);
+  if (!rows) return fail(MQ_EINVAL, "null rows");
+  uint32_t cols[32];
+  int rc = rows_to_cols(h, rows, c, cols);
+  if (rc) return rc;
   DeviceGuard g(h->device);
   return launch_affine_cols(h, cols, (uint32_t)c);
   MQ_TRY_END

@@ -281,6 +281,54 @@ static int launch_diag_pass(mq_state* h, const std::vector<PlannedLut>& in_luts)
   return MQ_OK;
 }
 
+// The diagonal as contiguous-window tables for a tile-sweep epilogue (the
+// fused layer of mq_tile.cu): same factorisation as launch_diag_terms, with
+// the global phase folded into the first table.  out.n = -1 when no plan with
+// <= 8 contiguous windows and <= max_entries entries exists.
+int plan_diag_windows(mq_state* h, int n_terms, const int32_t* kinds, const int32_t* wires, const double* params,
+                      int max_entries, DiagWindows& out) {
+  std::vector<Term> terms;
+  std::complex<double> scalar;
+  int rc = build_terms(h->n, n_terms, kinds, wires, params, terms, scalar);
+  if (rc) return rc;
+  out = DiagWindows();
+  out.n = -1;
+  for (int W = 10; W >= 1; --W) {
+    std::vector<PlannedLut> luts = plan_luts(terms, W);
+    size_t entries = 0;
+    bool contig = true;
+    for (auto& L : luts) {
+      entries += L.vals.size();
+      contig = contig && L.contig && !L.pos.empty();
+    }
+    if (!contig || (int)luts.size() > kMaxLuts) continue;
+    if (luts.empty()) {
+      PlannedLut L;
+      L.pos = {0};
+      L.contig = true;
+      L.vals = {1.0, 1.0};
+      luts.push_back(L);
+      entries = 2;
+    }
+    if ((int)entries > max_entries) continue;
+    for (auto& v : luts[0].vals) v *= scalar;
+    out.n = (int)luts.size();
+    uint32_t off = 0;
+    for (int l = 0; l < out.n; ++l) {
+      out.shift[l] = luts[l].pos[0];
+      out.nbits[l] = (int)luts[l].pos.size();
+      out.off[l] = (int)off;
+      for (auto v : luts[l].vals) {
+        out.vals.push_back(v.real());
+        out.vals.push_back(v.imag());
+      }
+      off += (uint32_t)luts[l].vals.size();
+    }
+    break;
+  }
+  return MQ_OK;
+}
+
 int launch_diag_terms(mq_state* h, int n_terms, const int32_t* kinds, const int32_t* wires, const double* params) {
   std::vector<Term> terms;
   std::complex<double> scalar;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <vector>
 
 #include "../../include/mq.h"
 
@@ -116,6 +117,21 @@ int launch_cu2_list(mq_state* h, int n_gates, const int32_t* targets, const uint
 // Diagonal layers (mq_diag.cu)
 int launch_diag_terms(mq_state* h, int n_terms, const int32_t* kinds, const int32_t* wires,
                       const double* params);
+// A diagonal factored into <= 8 tables indexed by contiguous index windows:
+// phase(x) = prod_w vals[off[w] + ((x >> shift[w]) & (2^nbits[w] - 1))]
+// (vals: re, im interleaved).  Planned by mq_diag.cu for tile epilogues.
+struct DiagWindows {
+  int n = 0;  // -1: not representable within the budget
+  int shift[8] = {}, nbits[8] = {}, off[8] = {};
+  std::vector<double> vals;
+};
+int plan_diag_windows(mq_state* h, int n_terms, const int32_t* kinds, const int32_t* wires, const double* params,
+                      int max_entries, DiagWindows& out);
+// Fused layer: U(2) on every active qubit, then the diagonal terms, then the
+// GF(2) permutation out[y] = in[A y ^ c] (cols = A e_j; null = none)
+// (mq_tile.cu).
+int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_terms, const int32_t* kinds,
+                 const int32_t* wires, const double* params, const uint32_t* cols, uint32_t c);
 // GF(2) affine permutation, out-of-place into the alternate buffer (mq_perm.cu).
 // cols[j] = A e_j (index-bit columns of the source map), c = flip constant.
 int launch_affine_cols(mq_state* h, const uint32_t* cols, uint32_t c);

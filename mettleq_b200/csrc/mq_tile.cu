@@ -81,6 +81,30 @@ struct TileParams {
   TileOp ops[kMaxOps];
 };
 
+// Epilogue of the fused layer's low sweep (tile = index bits [0, M)): after
+// the U(2) phases, every amplitude x of the tile is multiplied by the
+// diagonal phase(x) = prod_w lut[off[w] + ((x >> shift[w]) & (2^nbits[w]-1))]
+// and, with a permutation out[y] = in[A y ^ c] whose matrix maps the low
+// space span(e_0..e_{M-1}) onto itself, written to its output position.
+// Windows [0, n_var) overlap the tile bits; [n_var, n_win) are constant
+// over a tile and multiplied once per tile.
+constexpr int kEpiWin = 8;
+constexpr int kEpiLutBytes = 16384;
+struct EpiDesc {
+  uint8_t diag, perm, n_win, n_var;
+  uint8_t shift[kEpiWin];
+  uint8_t nbits[kEpiWin];
+  uint16_t off[kEpiWin];
+  uint32_t n_entries;  // table entries (complex values of the state's type)
+  uint32_t c;          // permutation flip constant
+  uint32_t cols[32];   // permutation columns A e_j
+  alignas(16) unsigned char lut[kEpiLutBytes];
+};
+struct FusedParams : TileParams {
+  EpiDesc epi;
+};
+static_assert(sizeof(FusedParams) <= 32000, "kernel parameter block too large");
+
 // e^{i pi L / 2^width}, 1 <= width <= 31, L < 2^width.
 template <typename R> struct Twiddle;
 template <> struct Twiddle<float> {
@@ -199,6 +223,71 @@ __device__ __forceinline__ void apply_qft_op(V2<R> (&a)[1 << LR], const TileOp& 
   }
 }
 
+// Shared-memory slot of tile-local amplitude i (the chunk swizzle of k_tile
+// at amplitude granularity).
+template <typename R>
+__device__ __forceinline__ uint32_t amp_slot(uint32_t i) {
+  return sizeof(R) == 4 ? (i ^ ((i >> 3) & 0xEu)) : (i ^ ((i >> 3) & 7u));
+}
+
+template <typename R>
+__device__ __forceinline__ V2<R> epi_phase(const EpiDesc& D, const V2<R>* lut, uint32_t x, V2<R> f) {
+#pragma unroll
+  for (int w = 0; w < kEpiWin; ++w) {
+    if (w >= D.n_var) break;
+    f = cmul(f, lut[D.off[w] + ((x >> D.shift[w]) & ((1u << D.nbits[w]) - 1u))]);
+  }
+  return f;
+}
+
+// MODE 2 write-back: output chunk c = tid + k*NT of output tile bo holds
+// amplitudes y = c << CB (and y | 1 for complex64); their values are the
+// processed input amplitudes l = cl ^ A y (identity without a permutation)
+// of input tile ib, times phase(ib | l).
+template <typename R, int M, int LT, int CPT>
+__device__ __forceinline__ void epilogue_store(const EpiDesc& D, const V2<R>* cur, const uint32_t* cols,
+                                               const V2<R>* lut, V2<R>* dst, uint32_t bo, uint32_t ib, uint32_t cl,
+                                               int tid) {
+  using T = V2<R>;
+  constexpr int NT = 1 << LT;
+  constexpr int CB = sizeof(T) == 8 ? 1 : 0;
+  constexpr int LCH = (M - CB) - LT;
+  const bool perm = D.perm, diag = D.diag;
+  uint32_t at = 0;
+  if (perm) {
+#pragma unroll
+    for (int b = 0; b < LT; ++b)
+      if ((tid >> b) & 1) at ^= cols[CB + b];
+  }
+  T hc = mk<R>(1, 0);
+  if (diag) {
+    for (int w = D.n_var; w < D.n_win; ++w)
+      hc = cmul(hc, lut[D.off[w] + ((ib >> D.shift[w]) & ((1u << D.nbits[w]) - 1u))]);
+  }
+#pragma unroll
+  for (int k = 0; k < CPT; ++k) {
+    const uint32_t y = ((uint32_t)tid + (uint32_t)(k * NT)) << CB;
+    uint32_t l0 = y;
+    if (perm) {
+      uint32_t ak = 0;
+#pragma unroll
+      for (int b = 0; b < LCH; ++b)
+        if ((k >> b) & 1) ak ^= cols[CB + LT + b];
+      l0 = cl ^ at ^ ak;
+    }
+    T v0 = cur[amp_slot<R>(l0)];
+    if (diag) v0 = cmul(v0, epi_phase<R>(D, lut, ib | l0, hc));
+    if constexpr (CB == 1) {
+      const uint32_t l1 = perm ? (l0 ^ cols[0]) : (y | 1u);
+      T v1 = cur[amp_slot<R>(l1)];
+      if (diag) v1 = cmul(v1, epi_phase<R>(D, lut, ib | l1, hc));
+      *reinterpret_cast<float4*>(dst + (bo | y)) = make_float4((float)v0.x, (float)v0.y, (float)v1.x, (float)v1.y);
+    } else {
+      dst[bo | y] = v0;
+    }
+  }
+}
+
 template <int M>
 __device__ __forceinline__ uint32_t tile_base_of(uint32_t tile, const TileParams& P) {
   uint64_t x = tile;
@@ -221,10 +310,15 @@ __device__ __forceinline__ uint32_t tile_base_of(uint32_t tile, const TileParams
 // per-bit slots (PhaseDesc s_reg / s_grp) and the kernel combines them with
 // XOR.  Without it, a register phase over tile bits 0-3 (the low sweep) has
 // the 16 threads of a half-warp 128 bytes apart, all in one bank pair.
-template <typename R, int M, int LR, int LT, bool QFT>
+//
+// MODE 0: U(2) / controlled U(2) phases; MODE 1: QFT stages; MODE 2: U(2)
+// phases plus the fused-layer epilogue (PT = FusedParams, tile bits [0, M)).
+template <typename R, int M, int LR, int LT, int MODE, typename PT>
 __global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? 3 : (LT >= 7 ? (sizeof(R) == 4 && LR == 4 ? 6 : 3) : (LT >= 6 && sizeof(R) == 4 ? 8 : 1)))))
-k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
+k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   using T = V2<R>;
+  constexpr bool QFT = MODE == 1;
+  constexpr bool EPI = MODE == 2;
   constexpr int NT = 1 << LT;
   constexpr int NR = 1 << LR;
   constexpr int E = 1 << M;
@@ -238,11 +332,21 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
   T* bufs = reinterpret_cast<T*>(smem_raw);
   PhaseDesc* phs = reinterpret_cast<PhaseDesc*>(smem_raw + 2 * sizeof(T) * E);
   float2* tw = reinterpret_cast<float2*>(smem_raw + 2 * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases);
+  // MODE 2: permutation columns, then the diagonal tables
+  uint32_t* ecols = reinterpret_cast<uint32_t*>(smem_raw + 2 * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases);
+  T* elut = reinterpret_cast<T*>(smem_raw + 2 * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases + 128);
   const int tid = threadIdx.x;
   {
     const uint32_t words = (uint32_t)(sizeof(PhaseDesc) * P.n_phases / 4);
     const uint32_t* srcw = reinterpret_cast<const uint32_t*>(&P.ph[0]);
     uint32_t* dstw = reinterpret_cast<uint32_t*>(phs);
+    for (uint32_t w = tid; w < words; w += NT) dstw[w] = srcw[w];
+  }
+  if constexpr (EPI) {
+    for (int w = tid; w < 32; w += NT) ecols[w] = P.epi.cols[w];
+    const uint32_t words = P.epi.n_entries * (uint32_t)(sizeof(T) / 4);
+    const uint32_t* srcw = reinterpret_cast<const uint32_t*>(P.epi.lut);
+    uint32_t* dstw = reinterpret_cast<uint32_t*>(elut);
     for (uint32_t w = tid; w < words; w += NT) dstw[w] = srcw[w];
   }
   __syncthreads();
@@ -281,9 +385,27 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
     return g;
   };
 
+  // Source tile of output tile t.  MODE 2 with a permutation: the output
+  // tile t << M reads A (t << M) ^ c, a whole input tile plus a low offset
+  // (returned in cl) because A maps the low space onto itself.
+  auto src_base = [&](uint32_t t, uint32_t& cl) -> uint32_t {
+    cl = 0;
+    if constexpr (EPI) {
+      const uint32_t bo = t << M;
+      if (!P.epi.perm) return bo;
+      uint32_t b = P.epi.c;
+      for (int j = M; j < (int)P.n; ++j)
+        if ((bo >> j) & 1u) b ^= ecols[j];
+      cl = b & (uint32_t)(E - 1);
+      return b & ~(uint32_t)(E - 1);
+    } else {
+      return tile_base_of<M>(t, P);
+    }
+  };
   uint32_t tile = blockIdx.x;
   if (tile < P.n_tiles) {
-    const uint32_t gb = tile_base_of<M>(tile, P) | g_t;
+    uint32_t cl;
+    const uint32_t gb = src_base(tile, cl) | g_t;
     const uint32_t sb = smem_u32(bufs);
 #pragma unroll
     for (int k = 0; k < CPT; ++k) cp_async<16>(sb + 16u * slot(k), src + (gb | g_k(k)));
@@ -295,7 +417,8 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
     T* cur = bufs + (it & 1) * E;
     const uint32_t next = tile + gridDim.x;
     if (next < P.n_tiles) {
-      const uint32_t gb = tile_base_of<M>(next, P) | g_t;
+      uint32_t cl;
+      const uint32_t gb = src_base(next, cl) | g_t;
       const uint32_t sb = smem_u32(bufs + ((it + 1) & 1) * E);
 #pragma unroll
       for (int k = 0; k < CPT; ++k) cp_async<16>(sb + 16u * slot(k), src + (gb | g_k(k)));
@@ -303,7 +426,8 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
-    const uint32_t base = tile_base_of<M>(tile, P);
+    uint32_t cl_in;
+    const uint32_t base = src_base(tile, cl_in);
     for (int ph = 0; ph < P.n_phases; ++ph) {
       const PhaseDesc& D = phs[ph];
       uint32_t greg[LR], sreg[LR];
@@ -348,6 +472,11 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ TileParams P) {
         }
       }
       __syncthreads();
+    }
+    if constexpr (EPI) {
+      epilogue_store<R, M, LT, CPT>(P.epi, cur, ecols, elut, dst, tile << M, base, cl_in, tid);
+      __syncthreads();
+      continue;
     }
     const uint32_t gb = base | g_t;
     const float4* c4 = reinterpret_cast<const float4*>(cur);
@@ -427,9 +556,9 @@ static void make_phases(int m, int lr, const std::vector<int>& order, Sweep& sw,
   }
 }
 
-template <typename R, int M, int LR, int LT, bool QFT>
-static int launch_tile_t(mq_state* h, const TileParams& P, size_t smem, bool out_of_place) {
-  auto kern = k_tile<R, M, LR, LT, QFT>;
+template <typename R, int M, int LR, int LT, int MODE, typename PT>
+static int launch_tile_t(mq_state* h, const PT& P, size_t smem, bool out_of_place) {
+  auto kern = k_tile<R, M, LR, LT, MODE, PT>;
   static int configured_smem = -1;
   static int blocks_per_sm = 0;
   if ((int)smem > configured_smem) {
@@ -449,14 +578,14 @@ static int launch_tile_t(mq_state* h, const TileParams& P, size_t smem, bool out
   return MQ_OK;
 }
 
-template <typename R, bool QFT, int LR>
-static int dispatch_tile_lr(mq_state* h, const TileParams& P, size_t smem) {
+template <typename R, int MODE, int LR, typename PT>
+static int dispatch_tile_lr(mq_state* h, const PT& P, size_t smem, bool oop) {
   switch (P.m) {
 #define MQ_TILE_CASE(MM)                                                        \
     case MM: {                                                                  \
       constexpr int L = (MM) < LR ? (MM) : LR;                                  \
       constexpr int LT = ((MM) - L) < 8 ? ((MM) - L) : 8;                       \
-      return launch_tile_t<R, MM, L, LT, QFT>(h, P, smem, false);              \
+      return launch_tile_t<R, MM, L, LT, MODE, PT>(h, P, smem, oop);            \
     }
     MQ_TILE_CASE(1) MQ_TILE_CASE(2) MQ_TILE_CASE(3) MQ_TILE_CASE(4) MQ_TILE_CASE(5) MQ_TILE_CASE(6)
     MQ_TILE_CASE(7) MQ_TILE_CASE(8) MQ_TILE_CASE(9) MQ_TILE_CASE(10) MQ_TILE_CASE(11)
@@ -464,35 +593,86 @@ static int dispatch_tile_lr(mq_state* h, const TileParams& P, size_t smem) {
     case 12:
       if constexpr (sizeof(R) == 4) {
         constexpr int LT = LR == 5 ? 7 : 8;
-        return launch_tile_t<R, 12, LR, LT, QFT>(h, P, smem, false);
+        return launch_tile_t<R, 12, LR, LT, MODE, PT>(h, P, smem, oop);
       }
       break;
     case 13:
-      if constexpr (sizeof(R) == 4 && LR == 4) return launch_tile_t<R, 13, 4, 9, QFT>(h, P, smem, false);
+      if constexpr (sizeof(R) == 4 && LR == 4) return launch_tile_t<R, 13, 4, 9, MODE, PT>(h, P, smem, oop);
       break;
     default: break;
   }
   return fail(MQ_EUNSUPPORTED, "tile size not instantiated");
 }
 
-template <typename R, bool QFT>
-static int dispatch_tile(mq_state* h, const TileParams& P, size_t smem) {
-  if constexpr (sizeof(R) == 4) {
-    if (reg_bits(MQ_C64, 12) == 4) return dispatch_tile_lr<R, QFT, 4>(h, P, smem);
-    return dispatch_tile_lr<R, QFT, 5>(h, P, smem);
+template <typename R, int MODE, typename PT>
+static int dispatch_tile(mq_state* h, const PT& P, size_t smem, bool oop) {
+  if constexpr (MODE == 2) {
+    return dispatch_tile_lr<R, MODE, 4>(h, P, smem, oop);
+  } else {
+    if constexpr (sizeof(R) == 4) {
+      if (reg_bits(MQ_C64, 12) == 4) return dispatch_tile_lr<R, MODE, 4>(h, P, smem, oop);
+      return dispatch_tile_lr<R, MODE, 5>(h, P, smem, oop);
+    }
+    return dispatch_tile_lr<R, MODE, 4>(h, P, smem, oop);
   }
-  return dispatch_tile_lr<R, QFT, 4>(h, P, smem);
 }
 
-static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, const std::vector<int>& op_rk) {
+// Fused-layer epilogue of a low sweep (see EpiDesc).
+struct EpiPlan {
+  bool diag = false, perm = false;
+  DiagWindows win;
+  uint32_t cols[32] = {};
+  uint32_t c = 0;
+};
+
+template <typename R>
+static void fill_epi(EpiDesc& D, const EpiPlan& e, int m, int n) {
+  D.diag = e.diag ? 1 : 0;
+  D.perm = e.perm ? 1 : 0;
+  if (e.perm) {
+    for (int j = 0; j < n; ++j) D.cols[j] = e.cols[j];
+    D.c = e.c;
+  }
+  if (!e.diag) return;
+  // windows overlapping the tile bits [0, m) first
+  std::vector<int> order;
+  for (int w = 0; w < e.win.n; ++w)
+    if (e.win.shift[w] < m) order.push_back(w);
+  D.n_var = (uint8_t)order.size();
+  for (int w = 0; w < e.win.n; ++w)
+    if (e.win.shift[w] >= m) order.push_back(w);
+  D.n_win = (uint8_t)order.size();
+  R* vals = reinterpret_cast<R*>(D.lut);
+  uint32_t off = 0;
+  for (size_t i = 0; i < order.size(); ++i) {
+    const int w = order[i];
+    D.shift[i] = (uint8_t)e.win.shift[w];
+    D.nbits[i] = (uint8_t)e.win.nbits[w];
+    D.off[i] = (uint16_t)off;
+    const uint32_t cnt = 1u << e.win.nbits[w];
+    for (uint32_t j = 0; j < cnt; ++j) {
+      vals[2 * (off + j)] = (R)e.win.vals[2 * (e.win.off[w] + j)];
+      vals[2 * (off + j) + 1] = (R)e.win.vals[2 * (e.win.off[w] + j) + 1];
+    }
+    off += cnt;
+  }
+  D.n_entries = off;
+}
+
+static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, const std::vector<int>& op_rk,
+                     const EpiPlan* epi = nullptr) {
   const int m = (int)sw.tile_bits.size();
-  const int lr = reg_bits(h->dtype, m);
+  const int lr = epi ? std::min(m, 4) : reg_bits(h->dtype, m);
   if (m < 1 || m > tile_max(h->dtype) || m > h->n) return fail(MQ_EINVAL, "bad tile size");
   if (sw.tile_bits[0] != 0) return fail(MQ_EINVAL, "tile must contain index bit 0");
   if ((int)sw.ops.size() > kMaxOps || (int)sw.phases.size() > kMaxPhases) return fail(MQ_EINVAL, "tile plan too large");
+  if (epi)
+    for (int k = 0; k < m; ++k)
+      if (sw.tile_bits[k] != k) return fail(MQ_EINVAL, "fused epilogue needs the low tile [0, m)");
   const bool qft = !sw.ops.empty() && (sw.ops[0].kind == OP_QFT_FWD || sw.ops[0].kind == OP_QFT_INV);
-  TileParams P;
-  std::memset(&P, 0, sizeof(P));
+  FusedParams F;
+  std::memset(&F, 0, sizeof(F));
+  TileParams& P = F;
   P.n_tiles = (uint32_t)(uint64_t(1) << (h->n - m));
   P.n = (uint8_t)h->n;
   P.m = (uint8_t)m;
@@ -561,8 +741,17 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
   P.scale = sw.has_scale ? sw.scale : 1.0;
   size_t smem = 2 * (h->amp_bytes() << m) + sizeof(PhaseDesc) * kMaxPhases;
   if (P.need_tw) smem += 3072 * sizeof(float2);
-  if (h->dtype == MQ_C64) return qft ? dispatch_tile<float, true>(h, P, smem) : dispatch_tile<float, false>(h, P, smem);
-  return qft ? dispatch_tile<double, true>(h, P, smem) : dispatch_tile<double, false>(h, P, smem);
+  if (epi) {
+    if (qft) return fail(MQ_EINVAL, "fused epilogue on a QFT sweep");
+    if (h->dtype == MQ_C64) fill_epi<float>(F.epi, *epi, m, h->n);
+    else fill_epi<double>(F.epi, *epi, m, h->n);
+    smem += 128 + (size_t)F.epi.n_entries * h->amp_bytes();
+    if (h->dtype == MQ_C64) return dispatch_tile<float, 2>(h, F, smem, epi->perm);
+    return dispatch_tile<double, 2>(h, F, smem, epi->perm);
+  }
+  if (h->dtype == MQ_C64)
+    return qft ? dispatch_tile<float, 1>(h, P, smem, false) : dispatch_tile<float, 0>(h, P, smem, false);
+  return qft ? dispatch_tile<double, 1>(h, P, smem, false) : dispatch_tile<double, 0>(h, P, smem, false);
 }
 
 static int tile_local(const std::vector<int>& bits, int gbit) {
@@ -606,38 +795,106 @@ static std::vector<std::pair<int, int>> split_bits(int n, int tmax, int pas) {
   return groups;
 }
 
-int launch_u2_layer(mq_state* h, const double* mats, const uint8_t* active) {
+// The U(2) sweep of index bits [start, start+cnt): targets are the active
+// qubits among them.  Returns false when none is active.
+static bool build_u2_sweep(mq_state* h, const double* mats, const uint8_t* active, int start, int cnt, Sweep& sw,
+                           std::vector<int>& op_phase, std::vector<int>& op_rk) {
   const int n = h->n;
-  const int tmax = tile_max(h->dtype);
-  const int pas = passengers();
-  for (auto [start, cnt] : split_bits(n, tmax, pas)) {
-    std::vector<int> gbits;
-    std::vector<int> qubits;
-    for (int b = start + cnt - 1; b >= start; --b) {
-      const int q = n - 1 - b;
-      if (active && !active[q]) continue;
-      gbits.push_back(b);
-      qubits.push_back(q);
-    }
-    if (gbits.empty()) continue;
+  std::vector<int> gbits, qubits;
+  for (int b = start + cnt - 1; b >= start; --b) {
+    const int q = n - 1 - b;
+    if (active && !active[q]) continue;
+    gbits.push_back(b);
+    qubits.push_back(q);
+  }
+  if (gbits.empty()) return false;
+  sw.tile_bits = tile_for(n, gbits, passengers(), tile_max(h->dtype));
+  const int m = (int)sw.tile_bits.size();
+  const int lr = reg_bits(h->dtype, m);
+  std::vector<int> order;
+  for (int b : gbits) order.push_back(tile_local(sw.tile_bits, b));
+  make_phases(m, lr, order, sw, op_phase, op_rk);
+  for (size_t i = 0; i < order.size(); ++i) {
+    TileOp op;
+    std::memset(&op, 0, sizeof(op));
+    op.kind = OP_U2;
+    for (int j = 0; j < 8; ++j) op.u[j] = mats[(size_t)qubits[i] * 8 + j];
+    sw.ops.push_back(op);
+  }
+  return true;
+}
+
+int launch_u2_layer(mq_state* h, const double* mats, const uint8_t* active) {
+  for (auto [start, cnt] : split_bits(h->n, tile_max(h->dtype), passengers())) {
     Sweep sw;
-    sw.tile_bits = tile_for(n, gbits, pas, tmax);
-    const int m = (int)sw.tile_bits.size();
-    const int lr = reg_bits(h->dtype, m);
-    std::vector<int> order;
-    for (int b : gbits) order.push_back(tile_local(sw.tile_bits, b));
     std::vector<int> op_phase, op_rk;
-    make_phases(m, lr, order, sw, op_phase, op_rk);
-    for (size_t i = 0; i < order.size(); ++i) {
-      TileOp op;
-      std::memset(&op, 0, sizeof(op));
-      op.kind = OP_U2;
-      for (int j = 0; j < 8; ++j) op.u[j] = mats[(size_t)qubits[i] * 8 + j];
-      sw.ops.push_back(op);
-    }
+    if (!build_u2_sweep(h, mats, active, start, cnt, sw, op_phase, op_rk)) continue;
     int rc = run_sweep(h, sw, op_phase, op_rk);
     if (rc) return rc;
   }
+  return MQ_OK;
+}
+
+// One layer of the config-0 structure in as few sweeps as the U(2) layer
+// alone: U(2) on every active qubit, then the diagonal terms, then the GF(2)
+// permutation (the reference runs u2_list_layer_all, zz_weighted_layer and
+// xor_affine_gather as three kernels, device.py:1089-1097).  The high bit
+// groups run first as plain sweeps; the low group [0, m) runs last and, as
+// every other U(2) gate is applied by then, multiplies the diagonal into its
+// tile and writes through the permutation when A maps span(e_0..e_{m-1})
+// onto itself (CNOT ladders do).  A diagonal that does not factor into
+// contiguous windows, or a permutation that mixes the low bits with high
+// ones, runs as its own pass after the sweep.
+int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_terms, const int32_t* kinds,
+                 const int32_t* wires, const double* params, const uint32_t* cols, uint32_t c) {
+  const int n = h->n;
+  if (cols) {
+    uint32_t inv[32];
+    if (!gf2_invert(n, cols, inv)) return fail(MQ_EINVAL, "affine map is not invertible over GF(2)");
+  }
+  const auto groups = split_bits(n, tile_max(h->dtype), passengers());
+  // low sweep plan first, so that argument errors surface before any launch
+  Sweep low;
+  std::vector<int> low_phase, low_rk;
+  const bool low_u2 = mats && build_u2_sweep(h, mats, active, groups[0].first, groups[0].second, low, low_phase, low_rk);
+  if (!low_u2) low.tile_bits = tile_for(n, {0}, passengers(), tile_max(h->dtype));
+  const int m = (int)low.tile_bits.size();
+  EpiPlan e;
+  if (n_terms > 0) {
+    int rc = plan_diag_windows(h, n_terms, kinds, wires, params, kEpiLutBytes / (int)h->amp_bytes(), e.win);
+    if (rc) return rc;
+    e.diag = e.win.n > 0;
+  }
+  const bool diag_separate = n_terms > 0 && !e.diag;
+  if (cols && !diag_separate) {
+    e.perm = true;
+    for (int j = 0; j < m; ++j)
+      if (cols[j] >> m) e.perm = false;
+    if (e.perm) {
+      for (int j = 0; j < n; ++j) e.cols[j] = cols[j];
+      e.c = c;
+      int rc = ensure_alt(h);
+      if (rc) return rc;
+    }
+  }
+  if (mats) {
+    for (size_t g = 1; g < groups.size(); ++g) {
+      Sweep sw;
+      std::vector<int> op_phase, op_rk;
+      if (!build_u2_sweep(h, mats, active, groups[g].first, groups[g].second, sw, op_phase, op_rk)) continue;
+      int rc = run_sweep(h, sw, op_phase, op_rk);
+      if (rc) return rc;
+    }
+  }
+  if (low_u2 || e.diag || e.perm) {
+    int rc = run_sweep(h, low, low_phase, low_rk, (e.diag || e.perm) ? &e : nullptr);
+    if (rc) return rc;
+  }
+  if (diag_separate) {
+    int rc = launch_diag_terms(h, n_terms, kinds, wires, params);
+    if (rc) return rc;
+  }
+  if (cols && !e.perm) return launch_affine_cols(h, cols, c);
   return MQ_OK;
 }
 

@@ -94,6 +94,8 @@ class Device:
         sim = self.sim
         if name == "_U2LISTLAYER":
             sim.apply_u2_layer(layer["mats"], layer["active"])
+        elif name == "_LAYER":
+            sim.apply_layer(layer["mats"], layer["active"], layer["terms"], layer["rows"], layer["c"])
         elif name == "_DIAG":
             sim.apply_diag_terms(layer["terms"])
         elif name == "_XORLAYER":

@@ -35,6 +35,24 @@ def _mats_array(n: int, mats) -> np.ndarray:
     return np.ascontiguousarray(out)
 
 
+def _pack_terms(terms):
+    """Diagonal terms (kind, wire_a, wire_b, params) as the C arrays
+    kinds[k], wires[2k], params[8k]; (None, None, None) when empty."""
+    k = len(terms)
+    if k == 0:
+        return None, None, None
+    kinds = np.empty(k, dtype=np.int32)
+    wires = np.empty(2 * k, dtype=np.int32)
+    params = np.zeros((k, 8), dtype=np.float64)
+    for i, (kind, a, b, p) in enumerate(terms):
+        kinds[i] = int(kind)
+        wires[2 * i] = int(a)
+        wires[2 * i + 1] = int(b)
+        pp = list(p)
+        params[i, :len(pp)] = pp
+    return kinds, wires, params
+
+
 def pauli_masks(n: int, word: Dict[int, str]) -> Tuple[int, int, int]:
     """(xmask, zmask, ny) over index bits for a Pauli word {wire: 'X'|'Y'|'Z'|'I'}."""
     x = z = ny = 0
@@ -184,15 +202,7 @@ class StateVector:
         k = len(terms)
         if k == 0:
             return
-        kinds = np.empty(k, dtype=np.int32)
-        wires = np.empty(2 * k, dtype=np.int32)
-        params = np.zeros((k, 8), dtype=np.float64)
-        for i, (kind, a, b, p) in enumerate(terms):
-            kinds[i] = int(kind)
-            wires[2 * i] = int(a)
-            wires[2 * i + 1] = int(b)
-            pp = list(p)
-            params[i, :len(pp)] = pp
+        kinds, wires, params = _pack_terms(terms)
         self.param_bytes += kinds.nbytes + wires.nbytes + params.nbytes
         N.check(self._lib.mq_apply_diag_terms(self._h, k, _ptr(kinds), _ptr(wires), _ptr(params)))
 
@@ -233,6 +243,39 @@ class StateVector:
             raise ValueError("rows must have one mask per qubit")
         self.param_bytes += r.nbytes + 8
         N.check(self._lib.mq_apply_xor_affine(self._h, _ptr(r), int(c)))
+
+    # -- fused layer ----------------------------------------------------------
+    def apply_layer(self, mats=None, active: Optional[Iterable[int]] = None,
+                    terms: Sequence[Tuple[int, int, int, Sequence[float]]] = (),
+                    rows: Optional[Sequence[int]] = None, c: int = 0) -> None:
+        """U(2) on the active qubits, then the commuting diagonal ``terms``,
+        then the permutation out[y] = in[f^{-1}(y)] (inverse ``rows``/``c``),
+        in the sweeps of the U(2) layer alone where the diagonal and the
+        permutation allow it (one config-0 layer: u2_list_layer_all +
+        zz_weighted_layer + xor_affine_gather, device.py:1089-1097)."""
+        m = act = None
+        if mats is not None:
+            m = _mats_array(self.n, mats)
+            if active is not None:
+                act = np.zeros(self.n, dtype=np.uint8)
+                for q in active:
+                    if not (0 <= int(q) < self.n):
+                        raise ValueError("Qubit index out of range")
+                    act[int(q)] = 1
+        kinds, wires, params = _pack_terms(terms)
+        r = None
+        if rows is not None:
+            r = np.ascontiguousarray(np.asarray([int(x) for x in rows], dtype=np.uint64))
+            if r.size != self.n:
+                raise ValueError("rows must have one mask per qubit")
+        for a in (m, act, kinds, wires, params, r):
+            if a is not None:
+                self.param_bytes += a.nbytes
+        N.check(self._lib.mq_apply_layer(
+            self._h, _ptr(m) if m is not None else None, _ptr(act) if act is not None else None,
+            0 if kinds is None else int(kinds.size), _ptr(kinds) if kinds is not None else None,
+            _ptr(wires) if wires is not None else None, _ptr(params) if params is not None else None,
+            _ptr(r) if r is not None else None, int(c)))
 
     # -- (e) probabilities, sampling, expectations ------------------------
     def probabilities(self, wires: Optional[Sequence[int]] = None, dtype=np.float64) -> np.ndarray:

@@ -370,7 +370,41 @@ def fuse(operations: Sequence[dict], n: int, *, schedule: bool = True) -> List[D
             i += 1
             continue
         raise ValueError(f"Unsupported operation for the statevector engine: {name}")
-    return _merge(fused, n)
+    return fuse_layers(_merge(fused, n))
+
+
+def fuse_layers(layers: List[dict]) -> List[dict]:
+    """Combine a U(2) layer with the diagonal layer and / or permutation
+    that follow it (in that order), or a diagonal with the permutation after
+    it, into one ``_LAYER``: the engine applies the three in the sweeps of
+    the U(2) layer alone (one config-0 layer is u2_list_layer_all +
+    zz_weighted_layer + xor_affine_gather in the reference,
+    device.py:1089-1097)."""
+    out: List[dict] = []
+    i, N = 0, len(layers)
+    while i < N:
+        L = layers[i]
+        if L["name"] not in ("_U2LISTLAYER", "_DIAG"):
+            out.append(L)
+            i += 1
+            continue
+        fusedl = {"name": "_LAYER", "mats": None, "active": None, "terms": [], "rows": None, "c": 0}
+        j = i
+        if layers[j]["name"] == "_U2LISTLAYER":
+            fusedl["mats"], fusedl["active"] = layers[j]["mats"], layers[j]["active"]
+            j += 1
+        if j < N and layers[j]["name"] == "_DIAG":
+            fusedl["terms"] = layers[j]["terms"]
+            j += 1
+        if j < N and layers[j]["name"] == "_XORLAYER":
+            fusedl["rows"], fusedl["c"] = layers[j]["rows"], layers[j]["c"]
+            j += 1
+        if j - i >= 2:
+            out.append(fusedl)
+        else:
+            out.append(L)
+        i = max(j, i + 1)
+    return out
 
 
 def _window_layer(per_wire: Dict[int, np.ndarray], n: int) -> List[dict]:
@@ -440,28 +474,64 @@ def _merge(fused: List[dict], n: int) -> List[dict]:
     return out
 
 
+def _split_bits(n: int, tmax: int, pas: int) -> List[Tuple[int, int]]:
+    """Index-bit groups of the tile sweeps (mq_tile.cu split_bits)."""
+    if n <= tmax:
+        return [(0, n)]
+    hi_cap = tmax - pas
+    n_hi = -(-(n - tmax) // hi_cap)
+    low = max(n - n_hi * hi_cap, min(tmax, (n + n_hi) // (n_hi + 1)))
+    groups, start, rest = [(0, low)], low, n - low
+    for i in range(n_hi):
+        cnt = rest // n_hi + (1 if i < rest % n_hi else 0)
+        groups.append((start, cnt))
+        start += cnt
+    return groups
+
+
 def expected_sweeps(layer: dict, n: int, dtype: str = "complex64") -> int:
-    """Full-state passes a fused layer launches (for execution reports)."""
-    tmax = 13 if dtype == "complex64" else 12
-    kmax = min(10 if dtype == "complex64" else 8, tmax - 3)
+    """Full-state passes a fused layer launches (for execution reports), from
+    the engine's default tile plan (12-bit complex64 / 11-bit complex128
+    tiles, 4 low passenger bits)."""
+    tmax = 12 if dtype == "complex64" else 11
+    pas = 4
     name = layer["name"]
-    if name == "_U2LISTLAYER":
-        if n <= tmax:
-            return 1
-        s = -(-n // kmax)
-        groups, start = [], 0
-        for i in range(s):
-            cnt = n // s + (1 if i < n % s else 0)
-            groups.append((start, cnt))
-            start += cnt
-        bits = {n - 1 - q for q in layer["active"]}
+    groups = _split_bits(n, tmax, pas)
+
+    def u2_sweeps(active):
+        bits = {n - 1 - q for q in active}
         return sum(1 for st, cnt in groups if any(st <= b < st + cnt for b in bits))
+
+    if name == "_U2LISTLAYER":
+        return u2_sweeps(layer["active"])
+    if name == "_LAYER":
+        hi = u2_sweeps(layer["active"]) if layer["mats"] is not None else 0
+        low_bits = {n - 1 - q for q in (layer["active"] or [])}
+        m = min(n, max(groups[0][1], 10))
+        if layer["mats"] is not None and any(b < groups[0][1] for b in low_bits):
+            hi -= 1  # the low sweep is counted below
+        terms = layer["terms"]
+        far = any(b >= 0 and abs(a - b) >= 10 for _, a, b, _ in terms)
+        extra = 1 if far and terms else 0
+        perm_low = True
+        if layer["rows"] is not None:
+            rows = layer["rows"]
+            # columns A e_j for index bits j < m must stay below bit m
+            for j in range(m):
+                col = 0
+                for k, r in enumerate(rows):
+                    if (r >> j) & 1:
+                        col |= 1 << (n - 1 - k)
+                if col >> m:
+                    perm_low = False
+            if not perm_low or extra:
+                extra += 1
+        return hi + 1 + extra
     if name in ("_DIAG", "_XORLAYER"):
         return 1
     if name == "_QFTSTAGES":
         cnt = layer["j_end"] - layer["j_begin"]
-        kq = min(8 if dtype == "complex64" else 6, tmax - 3)
-        return 1 if cnt + 3 <= tmax else -(-cnt // kq)
+        return 1 if cnt + pas <= tmax else -(-cnt // (tmax - pas))
     if name == "_CULIST":
         return max(1, len(layer["gates"]))
     return 1

@@ -194,35 +194,33 @@ def affine_gates(rows: List[int], c: int, n: int) -> List[dict]:
     return gates
 
 
-def run_circuit_layers(sv, circuit: Circuit, on_layer=None) -> None:
-    """Apply a circuit at the kernel level: U(2) layer, RZZ diagonal layer,
-    CNOT-ladder permutation, then the QFT / permutation layers."""
+def run_circuit_layers(sv, circuit: Circuit, on_layer=None, fused: bool = True) -> None:
+    """Apply a circuit at the kernel level.  Each config layer (U(2) layer,
+    RZZ diagonal, CNOT-ladder permutation) is one fused ``apply_layer`` call
+    (``fused=False``: the three layer calls), then the QFT / permutation
+    layers.  ``on_layer(kind, edge)`` brackets every call (edge 0 before,
+    1 after) with kind "layer" (or "u2" / "diag" / "xor"), "qft" or "xor"."""
     n = circuit.n
     bonds = [(i, i + 1) for i in range(n - 1)]
     ladder = cnot_ladder_rows(n)
+
+    def run(kind, fn):
+        if on_layer:
+            on_layer(kind, 0)
+        fn()
+        if on_layer:
+            on_layer(kind, 1)
+
+    from .fusion import DIAG_ZZ
     for L in circuit.layers:
-        if on_layer:
-            on_layer("u2", 0)
-        sv.apply_u2_layer(L.mats)
-        if on_layer:
-            on_layer("u2", 1)
-            on_layer("diag", 0)
-        sv.apply_zz_weighted(bonds, [t / 2.0 for t in L.thetas])
-        if on_layer:
-            on_layer("diag", 1)
-            on_layer("xor", 0)
-        sv.apply_xor_affine(*ladder)
-        if on_layer:
-            on_layer("xor", 1)
+        if fused:
+            terms = [(DIAG_ZZ, i, i + 1, [t / 2.0]) for i, t in enumerate(L.thetas)]
+            run("layer", lambda: sv.apply_layer(L.mats, None, terms, *ladder))
+        else:
+            run("u2", lambda: sv.apply_u2_layer(L.mats))
+            run("diag", lambda: sv.apply_zz_weighted(bonds, [t / 2.0 for t in L.thetas]))
+            run("xor", lambda: sv.apply_xor_affine(*ladder))
         if L.qft_after:
-            if on_layer:
-                on_layer("qft", 0)
-            sv.apply_qft(None)
-            if on_layer:
-                on_layer("qft", 1)
+            run("qft", lambda: sv.apply_qft(None))
         if L.xor is not None:
-            if on_layer:
-                on_layer("xor", 0)
-            sv.apply_xor_affine(*L.xor)
-            if on_layer:
-                on_layer("xor", 1)
+            run("xor", lambda: sv.apply_xor_affine(*L.xor))

@@ -33,3 +33,29 @@ def random_invertible_rows(n: int, rng: np.random.Generator):
                 basis.append(r)
         if len(basis) == n:
             return rows
+
+
+def oracle_apply_terms(o, terms) -> None:
+    """Apply fused diagonal terms (kind, a, b, params) with the oracle's
+    per-gate routines (kinds as in mettleq_b200.fusion.DIAG_*)."""
+    from mettleq_b200 import fusion as F
+    for kind, a, b, p in terms:
+        t = p[0] if p else 0.0
+        if kind == F.DIAG_ZZ:
+            o.apply_zz_phase(t, a, b)
+        elif kind == F.DIAG_CPHASE:
+            o.apply_diagonal([1, 1, 1, np.exp(1j * t)], [a, b])
+        elif kind == F.DIAG_CRZ:
+            o.apply_diagonal([1, 1, np.exp(-0.5j * t), np.exp(0.5j * t)], [a, b])
+        elif kind == F.DIAG_RZ:
+            o.apply_diagonal([np.exp(-0.5j * t), np.exp(0.5j * t)], [a])
+        elif kind == F.DIAG_PHASE:
+            o.apply_diagonal([1, np.exp(1j * t)], [a])
+        elif kind == F.DIAG_1Q:
+            o.apply_diagonal([p[0] + 1j * p[1], p[2] + 1j * p[3]], [a])
+        elif kind == F.DIAG_2Q:
+            o.apply_diagonal([p[2 * i] + 1j * p[2 * i + 1] for i in range(4)], [a, b])
+        elif kind == F.DIAG_GLOBAL:
+            o.apply_global_phase(t)
+        else:
+            raise AssertionError(kind)

@@ -13,7 +13,7 @@ import pytest
 from mettleq_b200 import fusion as F
 from mettleq_b200 import workloads as W
 from oracle import OracleSim, compose_inverse_affine
-from tests.helpers import rand_state
+from tests.helpers import oracle_apply_terms, rand_state
 
 
 def interpret(layers, n, vec):
@@ -25,24 +25,14 @@ def interpret(layers, n, vec):
             for q in L["active"]:
                 o.apply_single(L["mats"][q].reshape(2, 2), q)
         elif name == "_DIAG":
-            for kind, a, b, p in L["terms"]:
-                t = p[0] if p else 0.0
-                if kind == F.DIAG_ZZ:
-                    o.apply_zz_phase(t, a, b)
-                elif kind == F.DIAG_CPHASE:
-                    o.apply_diagonal([1, 1, 1, np.exp(1j * t)], [a, b])
-                elif kind == F.DIAG_CRZ:
-                    o.apply_diagonal([1, 1, np.exp(-0.5j * t), np.exp(0.5j * t)], [a, b])
-                elif kind == F.DIAG_RZ:
-                    o.apply_diagonal([np.exp(-0.5j * t), np.exp(0.5j * t)], [a])
-                elif kind == F.DIAG_PHASE:
-                    o.apply_diagonal([1, np.exp(1j * t)], [a])
-                elif kind == F.DIAG_1Q:
-                    o.apply_diagonal([p[0] + 1j * p[1], p[2] + 1j * p[3]], [a])
-                elif kind == F.DIAG_2Q:
-                    o.apply_diagonal([p[2 * i] + 1j * p[2 * i + 1] for i in range(4)], [a, b])
-                elif kind == F.DIAG_GLOBAL:
-                    o.apply_global_phase(t)
+            oracle_apply_terms(o, L["terms"])
+        elif name == "_LAYER":
+            if L["mats"] is not None:
+                for q in L["active"]:
+                    o.apply_single(L["mats"][q].reshape(2, 2), q)
+            oracle_apply_terms(o, L["terms"])
+            if L["rows"] is not None:
+                o.apply_affine(L["rows"], L["c"])
         elif name == "_XORLAYER":
             o.apply_affine(L["rows"], L["c"])
         elif name == "_QFTSTAGES":
@@ -145,7 +135,8 @@ def test_config_layer_structure_fuses_to_three_layers():
     c = W.plain_circuit(8, 3, seed=1)
     ops, gphase = c.ops()
     layers = F.fuse(ops, 8)
-    assert [L["name"] for L in layers] == ["_U2LISTLAYER", "_DIAG", "_XORLAYER"] * 3
+    assert [L["name"] for L in layers] == ["_LAYER"] * 3
+    assert all(L["mats"] is not None and L["terms"] and L["rows"] is not None for L in layers)
     vec = rand_state(8, 1, np.complex128)
     got = interpret(layers, 8, vec) * np.exp(1j * gphase)
     o = OracleSim(8, np.complex128)
@@ -164,7 +155,9 @@ def test_scale_circuit_fuses_to_logical_layers():
     c = W.scale_circuit(12, 20, seed=2)
     ops, gphase = c.ops()
     layers = F.fuse(ops, 12)
-    assert len(layers) == c.logical_layers()
+    # one fused layer per config layer, plus each QFT and permutation layer
+    n_extra = sum(1 for L in c.layers if L.qft_after) + sum(1 for L in c.layers if L.xor is not None)
+    assert len(layers) == len(c.layers) + n_extra
     vec = rand_state(12, 5, np.complex128)
     got = interpret(layers, 12, vec)
     assert np.max(np.abs(got - reference(ops, 12, vec))) < 1e-9
@@ -234,3 +227,26 @@ def test_validation_errors():
         F.fuse([{"name": "H", "wires": [3], "parameters": []}], 2)
     with pytest.raises(ValueError):
         F.fuse([{"name": "FOO", "wires": [0], "parameters": []}], 2)
+
+
+def test_fuse_layers_combinations():
+    u = {"name": "_U2LISTLAYER", "mats": np.zeros((3, 4)), "active": [0]}
+    d = {"name": "_DIAG", "terms": [(F.DIAG_RZ, 0, -1, [0.1])]}
+    x = {"name": "_XORLAYER", "rows": [4, 2, 1], "c": 1}
+    q = {"name": "_QFTSTAGES", "q0": 0, "k": 3, "j_begin": 0, "j_end": 3, "inverse": False}
+    names = lambda ls: [L["name"] for L in ls]  # noqa: E731
+    assert names(F.fuse_layers([u, d, x])) == ["_LAYER"]
+    assert names(F.fuse_layers([u, x, q])) == ["_LAYER", "_QFTSTAGES"]
+    assert names(F.fuse_layers([d, x, u])) == ["_LAYER", "_U2LISTLAYER"]
+    assert names(F.fuse_layers([x, u, q, d])) == ["_XORLAYER", "_U2LISTLAYER", "_QFTSTAGES", "_DIAG"]
+    L = F.fuse_layers([d, x])[0]
+    assert L["mats"] is None and L["rows"] == [4, 2, 1] and L["c"] == 1
+
+
+def test_expected_sweeps_of_fused_config_layer():
+    c = W.plain_circuit(30, 1, seed=0)
+    ops, _ = c.ops()
+    layers = F.fuse(ops, 30)
+    assert [L["name"] for L in layers] == ["_LAYER"]
+    # 30 index bits in four tile groups; diagonal and ladder ride on the low sweep
+    assert F.expected_sweeps(layers[0], 30) == 4

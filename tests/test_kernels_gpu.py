@@ -11,7 +11,7 @@ import pytest
 
 from oracle import OracleSim, compose_inverse_affine
 from oracle import sampler as osamp
-from tests.helpers import haar_u2, rand_state, random_invertible_rows
+from tests.helpers import haar_u2, oracle_apply_terms, rand_state, random_invertible_rows
 
 pytestmark = pytest.mark.gpu
 
@@ -251,6 +251,91 @@ def test_expval_pauli_words(dtype):
     ref = np.array([o.pauli_expectation(w) for w in words])
     tol = 1e-6 if dtype == np.complex64 else 1e-12
     assert np.max(np.abs(got - ref)) < tol
+
+
+def _layer_reference(n, vec, mats, active, terms, rows, c):
+    o = _oracle(n, np.complex128, vec)
+    if mats is not None:
+        for q in (range(n) if active is None else active):
+            o.apply_single(mats[q].reshape(2, 2), q)
+    oracle_apply_terms(o, terms)
+    if rows is not None:
+        o.apply_affine(rows, c)
+    return o.state
+
+
+def _ladder(n):
+    from mettleq_b200.workloads import cnot_ladder_rows
+    return cnot_ladder_rows(n)
+
+
+@pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
+@pytest.mark.parametrize("n", [3, 5, 12, 13, 17, 22])
+def test_fused_config_layer(n, dtype):
+    """U(2) on every qubit + RZZ chain + CNOT ladder in one apply_layer call
+    (diagonal and ladder on the last U(2) sweep) equals the three layers."""
+    from mettleq_b200 import fusion as F
+    rng = np.random.default_rng(300 + n)
+    mats = np.stack([haar_u2(rng).reshape(4) for _ in range(n)])
+    terms = [(F.DIAG_ZZ, i, i + 1, [float(rng.uniform(0, math.pi))]) for i in range(n - 1)]
+    rows, c = _ladder(n)
+    vec = rand_state(n, n + 1, dtype)
+    sv = _sv(n, dtype, vec)
+    s0 = sv.counters()[1]
+    sv.apply_layer(mats, None, terms, rows, c)
+    sweeps = sv.counters()[1] - s0
+    assert _err(sv.get(), _layer_reference(n, vec, mats, None, terms, rows, c)) <= TOL[dtype]
+    # as many sweeps as the U(2) layer alone
+    s1 = sv.counters()[1]
+    sv.apply_u2_layer(mats)
+    assert sweeps == sv.counters()[1] - s1
+
+
+@pytest.mark.parametrize("case", ["far_bond", "random_perm", "high_only", "no_u2", "perm_only", "mixed_terms",
+                                  "no_perm", "flip_ladder"])
+@pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
+def test_fused_layer_variants(case, dtype):
+    """Every combination, including the ones that fall back to separate
+    diagonal / permutation passes, equals the sequential reference."""
+    from mettleq_b200 import fusion as F
+    n = 17
+    rng = np.random.default_rng(11)
+    mats = np.stack([haar_u2(rng).reshape(4) for _ in range(n)])
+    active = None
+    terms = [(F.DIAG_ZZ, i, i + 1, [float(rng.uniform(0, math.pi))]) for i in range(n - 1)]
+    rows, c = _ladder(n)
+    if case == "far_bond":
+        terms = terms + [(F.DIAG_ZZ, 0, n - 1, [0.37])]
+    elif case == "random_perm":
+        rows = random_invertible_rows(n, rng)
+        c = int(rng.integers(0, 1 << n))
+    elif case == "high_only":
+        active = [0, 1, 2, 5]
+    elif case == "no_u2":
+        mats = None
+    elif case == "perm_only":
+        mats, terms = None, []
+    elif case == "mixed_terms":
+        terms = [(F.DIAG_CPHASE, 3, 4, [0.7]), (F.DIAG_RZ, 16, -1, [1.1]), (F.DIAG_GLOBAL, 0, -1, [0.3]),
+                 (F.DIAG_CRZ, 9, 7, [-0.4]), (F.DIAG_PHASE, 0, -1, [2.0])]
+    elif case == "no_perm":
+        rows = None
+    elif case == "flip_ladder":
+        c = int(rng.integers(0, 1 << n))
+    vec = rand_state(n, 5, dtype)
+    sv = _sv(n, dtype, vec)
+    sv.apply_layer(mats, active, terms, rows, c)
+    assert _err(sv.get(), _layer_reference(n, vec, mats, active, terms, rows, c)) <= TOL[dtype]
+
+
+def test_fused_layer_rejects_singular_rows_before_any_work():
+    n = 6
+    vec = rand_state(n, 2)
+    sv = _sv(n, np.complex64, vec)
+    mats = np.stack([np.eye(2).reshape(4) * 1j for _ in range(n)])
+    with pytest.raises(ValueError):
+        sv.apply_layer(mats, None, [], [1, 1, 4, 8, 16, 32], 0)
+    assert _err(sv.get(), vec) == 0.0
 
 
 def test_errors_map_to_python_exceptions():
