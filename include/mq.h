@@ -70,6 +70,8 @@ int mq_state_create(int n, int dtype, int device, void* stream, mq_state** out);
 int mq_state_destroy(mq_state* h);
 int mq_state_info(const mq_state* h, int* n, int* dtype, int* device);
 int mq_state_set_stream(mq_state* h, void* stream);
+/* The stream the handle launches on (its own or the caller's). */
+int mq_state_stream(const mq_state* h, void** out);
 int mq_state_reset(mq_state* h);                       /* sim.py:32-45 */
 int mq_state_set(mq_state* h, const void* host_amps);  /* 2^n amplitudes */
 int mq_state_get(mq_state* h, void* host_amps);
@@ -145,6 +147,23 @@ int mq_sample(mq_state* h, const int32_t* wires, int k, uint64_t seed,
  * out[2w+1] = im (integrations/_common.py:384-427). */
 int mq_expval_pauli(mq_state* h, int n_words, const uint64_t* xmask,
                     const uint64_t* zmask, const int32_t* ny, double* out);
+/* ---- differentiation: adjoint method ------------------------------------ */
+/* The reference differentiates by parameter shift, two circuit runs per
+ * parameter (integrations/qml.py:308-332); these two calls give the adjoint
+ * method.  Both handles: same n, dtype, device and stream.
+ * out = H psi for H = sum_w zcoef[w] Z(zmasks[w]) + sum_q xcoef[q] X_q
+ * (zmasks over index bits; xcoef NULL = no X part); energy (nullable) =
+ * Re <psi|H|psi>. */
+int mq_apply_pauli_sum(mq_state* psi, mq_state* out, int n_z, const uint64_t* zmasks,
+                       const double* zcoef, const double* xcoef, double* energy);
+/* One backward layer: for each listed qubit q_i and step s = 0, 1:
+ * grads[2i+s] = Im <lam|G|psi> with G = gens[2i+s] (0 none, 1 X, 2 Y, 3 Z)
+ * on q_i, then psi, lam <- mats[(2i+s)*8 ..] (2x2 complex128
+ * [u00,u01,u10,u11]) on q_i.  For a gate exp(-i t G / 2) applied last in
+ * the forward circuit, passing its inverse gives dE/dt. */
+int mq_adjoint_layer(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits,
+                     const int32_t* gens, const double* mats, double* grads);
+
 /* mq_expval_pauli without any device allocation.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc or cudaFree
  * in the middle of their work -- a serving loop that admits requests by

@@ -35,6 +35,7 @@ SIGNATURES = {
     "mq_state_destroy": (_I, [_P]),
     "mq_state_info": (_I, [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
     "mq_state_set_stream": (_I, [_P, _P]),
+    "mq_state_stream": (_I, [_P, C.POINTER(_P)]),
     "mq_state_reset": (_I, [_P]),
     "mq_state_set": (_I, [_P, _P]),
     "mq_state_get": (_I, [_P, _P]),
@@ -55,6 +56,8 @@ SIGNATURES = {
     "mq_sample": (_I, [_P, _P, _I, _U64, _U64, _I64, _P]),
     "mq_expval_pauli": (_I, [_P, _I, _P, _P, _P, _P]),
     "mq_expval_pauli_static": (_I, [_P, _I, _P, _P, _P, _P]),
+    "mq_apply_pauli_sum": (_I, [_P, _P, _I, _P, _P, _P, _P]),
+    "mq_adjoint_layer": (_I, [_P, _P, _I, _P, _P, _P, _P]),
 }
 
 

@@ -1,0 +1,607 @@
+// Adjoint-method gradients (the differentiation direction of the engine).
+//
+// The reference differentiates by parameter shift: two full circuit runs per
+// parameter (integrations/qml.py:308-332).  The adjoint method needs one
+// forward run, one application of the observable and one backward run that
+// un-applies the circuit from the final state, so no intermediate states are
+// stored:
+//
+//   psi = U_L ... U_1 |0>,  lam = H psi,  E = Re <psi|lam>
+//   backward, for every gate U = exp(-i t G / 2) from the last to the first:
+//     dE/dt = Im <lam|G|psi>       (psi, lam taken right after U)
+//     psi <- U^dag psi,  lam <- U^dag lam
+//
+// Gates of one layer act on different qubits and commute, and a unitary
+// applied to both psi and lam leaves <lam|G_q|psi> unchanged when it acts on
+// other qubits, so a whole layer is handled by tile sweeps over index-bit
+// groups (as the U(2) layer): k_adj streams tiles of psi and lam through
+// shared memory together and, for every target bit, accumulates the
+// gradient of each generator just before un-applying its gate.
+//
+//   k_hdiag: lam = D psi for the Z-word part of H (one pass)
+//   k_adj (build mode): lam += sum_q c_q X_q psi (tile sweeps)
+//   k_dot:   E = Re <psi|lam> (one pass)
+//   k_adj (backward mode): gradients + un-apply, per layer
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "mq_internal.cuh"
+
+namespace mq {
+
+enum : uint8_t { GEN_NONE = 0, GEN_X = 1, GEN_Y = 2, GEN_Z = 3, GEN_XADD = 4 };
+
+constexpr int kAdjLR = 4;           // register bits per phase, complex64 (complex128: 3)
+constexpr int kAdjMaxPhases = 4;    // up to 12 target bits per sweep
+constexpr int kAdjTileMax = 11;     // psi and lam tiles, double-buffered: 4 * 2^11 * 8 B (complex64)
+constexpr int kAdjSlots = kAdjMaxPhases * kAdjLR;
+constexpr int kAdjPartials = 2 * kAdjSlots;  // per block: one double per (slot, step)
+constexpr int kAdjMaxTargets = 12;
+
+struct AdjSlot {
+  uint8_t gen[2];      // generator whose gradient is taken before step s
+  uint8_t has_u[2];    // step s un-applies a 2x2 gate
+  uint8_t pad[4];
+  alignas(16) float uf[2][8];
+  alignas(16) double ud[2][8];  // GEN_XADD: ud[s][0] = coefficient
+};
+
+struct AdjPhase {
+  uint32_t s_reg[kAdjLR];
+  uint32_t s_grp[16];
+  AdjSlot slot[kAdjLR];
+};
+
+struct AdjParams {
+  uint32_t n_tiles;
+  uint8_t n, m, n_phases, store_psi;
+  uint8_t tile_bit[16];
+  uint8_t hi_contig, hi_shift, pad[6];
+  AdjPhase ph[kAdjMaxPhases];
+};
+
+template <typename R>
+__device__ __forceinline__ V2<R> slot_u(const AdjSlot& S, int s, int j) {
+  if constexpr (sizeof(R) == 4) return make_float2(S.uf[s][2 * j], S.uf[s][2 * j + 1]);
+  else return make_double2(S.ud[s][2 * j], S.ud[s][2 * j + 1]);
+}
+
+template <typename T>
+__device__ __forceinline__ T cmac(T u0, T x0, T u1, T x1) {
+  T r;
+  r.x = fma(u0.x, x0.x, fma(-u0.y, x0.y, fma(u1.x, x1.x, -u1.y * x1.y)));
+  r.y = fma(u0.x, x0.y, fma(u0.y, x0.x, fma(u1.x, x1.y, u1.y * x1.x)));
+  return r;
+}
+
+// Gradient partial of generator `gen` on register bit K, then the step's gate
+// on both register sets.
+template <typename R, int LR, int K>
+__device__ __forceinline__ void adj_slot(V2<R> (&a)[1 << LR], V2<R> (&b)[1 << LR], const AdjSlot& S,
+                                         R (&acc)[2]) {
+  using T = V2<R>;
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const int gen = S.gen[s];
+    if (gen != GEN_NONE && gen != GEN_XADD) {
+      R g = 0;
+#pragma unroll
+      for (int r = 0; r < (1 << LR); ++r) {
+        if (r & (1 << K)) continue;
+        const T x0 = a[r], x1 = a[r | (1 << K)], l0 = b[r], l1 = b[r | (1 << K)];
+        if (gen == GEN_Z) {
+          g += (l0.x * x0.y - l0.y * x0.x) - (l1.x * x1.y - l1.y * x1.x);
+        } else if (gen == GEN_Y) {
+          g += (l1.x * x0.x + l1.y * x0.y) - (l0.x * x1.x + l0.y * x1.y);
+        } else {
+          g += (l0.x * x1.y - l0.y * x1.x) + (l1.x * x0.y - l1.y * x0.x);
+        }
+      }
+      acc[s] += g;
+    }
+    if (gen == GEN_XADD) {
+      const R c = (R)S.ud[s][0];
+#pragma unroll
+      for (int r = 0; r < (1 << LR); ++r) {
+        if (r & (1 << K)) continue;
+        const T x0 = a[r], x1 = a[r | (1 << K)];
+        b[r].x += c * x1.x; b[r].y += c * x1.y;
+        b[r | (1 << K)].x += c * x0.x; b[r | (1 << K)].y += c * x0.y;
+      }
+    }
+    if (S.has_u[s]) {
+      const T u00 = slot_u<R>(S, s, 0), u01 = slot_u<R>(S, s, 1), u10 = slot_u<R>(S, s, 2), u11 = slot_u<R>(S, s, 3);
+#pragma unroll
+      for (int r = 0; r < (1 << LR); ++r) {
+        if (r & (1 << K)) continue;
+        const int r1 = r | (1 << K);
+        const T x0 = a[r], x1 = a[r1];
+        a[r] = cmac(u00, x0, u01, x1);
+        a[r1] = cmac(u10, x0, u11, x1);
+        const T y0 = b[r], y1 = b[r1];
+        b[r] = cmac(u00, y0, u01, y1);
+        b[r1] = cmac(u10, y0, u11, y1);
+      }
+    }
+  }
+}
+
+template <int LR>
+__device__ __forceinline__ uint32_t xsel(int r, const uint32_t* g) {
+  uint32_t o = 0;
+#pragma unroll
+  for (int k = 0; k < LR; ++k)
+    if (r & (1 << k)) o ^= g[k];
+  return o;
+}
+
+// Tiles of 2^M amplitudes of psi and lam, 2^LT threads, shared-memory layout
+// as k_tile (chunk c at slot c ^ ((c >> 3) & 7)); per-block gradient partials
+// (one double per phase slot and step) go to `partials`.
+template <typename R, int M, int LR, int LT>
+__global__ void __launch_bounds__(1 << LT)
+k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __restrict__ partials) {
+  using T = V2<R>;
+  constexpr int NT = 1 << LT;
+  constexpr int NR = 1 << LR;
+  constexpr int E = 1 << M;
+  constexpr int GPT = (E / NR) / NT;
+  constexpr int CB = sizeof(T) == 8 ? 1 : 0;
+  constexpr int NCH = E >> CB;
+  constexpr int CPT = NCH / NT;
+  constexpr int LCH = (M - CB) - LT;
+  static_assert(GPT >= 1 && CPT >= 1, "bad tile configuration");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* bufs = reinterpret_cast<T*>(smem_raw);  // [psi0, psi1, lam0, lam1]
+  constexpr int WS = NT < 32 ? NT : 32;  // lanes per warp in use
+  constexpr unsigned WMASK = WS == 32 ? 0xffffffffu : ((1u << WS) - 1u);
+  __shared__ double red[(NT + 31) / 32][kAdjPartials];
+  const int tid = threadIdx.x;
+  uint32_t g_t = 0;
+#pragma unroll
+  for (int b = 0; b < LT; ++b)
+    if ((tid >> b) & 1) g_t |= 1u << P.tile_bit[CB + b];
+  const uint32_t s_t = (uint32_t)tid ^ (((uint32_t)tid >> 3) & 7u);
+  auto slot = [&](int k) -> uint32_t {
+    const uint32_t kk = (uint32_t)(k * NT);
+    return s_t ^ (kk ^ ((kk >> 3) & 7u));
+  };
+  auto g_k = [&](int k) -> uint32_t {
+    if (P.hi_contig) return (uint32_t)k << P.hi_shift;
+    uint32_t g = 0;
+#pragma unroll
+    for (int b = 0; b < LCH; ++b)
+      if ((k >> b) & 1) g |= 1u << P.tile_bit[CB + LT + b];
+    return g;
+  };
+  auto base_of = [&](uint32_t tile) -> uint32_t {
+    uint64_t x = tile;
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+      const int pb = P.tile_bit[k];
+      x = ((x >> pb) << (pb + 1)) | (x & ((uint64_t(1) << pb) - 1));
+    }
+    return (uint32_t)x;
+  };
+  auto issue = [&](uint32_t tile, int which) {
+    const uint32_t gb = base_of(tile) | g_t;
+    const uint32_t sp = smem_u32(bufs + which * E), sl = smem_u32(bufs + (2 + which) * E);
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+      cp_async<16>(sp + 16u * slot(k), psi + (gb | g_k(k)));
+      cp_async<16>(sl + 16u * slot(k), lam + (gb | g_k(k)));
+    }
+  };
+  // per-thread gradient sums over this thread's tiles, in the state's type
+  // (a few dozen terms each); blocks reduce them in double
+  constexpr int MAXPH = (12 + LR - 1) / LR < kAdjMaxPhases ? (12 + LR - 1) / LR : kAdjMaxPhases;
+  static_assert(MAXPH <= kAdjMaxPhases, "too many phases");
+  R acc[MAXPH][LR][2];
+#pragma unroll
+  for (int p = 0; p < MAXPH; ++p)
+#pragma unroll
+    for (int k = 0; k < LR; ++k) acc[p][k][0] = acc[p][k][1] = 0;
+
+  uint32_t tile = blockIdx.x;
+  if (tile < P.n_tiles) issue(tile, 0);
+  cp_async_commit();
+  T a[NR], b[NR];
+  for (int it = 0; tile < P.n_tiles; tile += gridDim.x, ++it) {
+    const int cb = it & 1;
+    T* cp = bufs + cb * E;
+    T* cl = bufs + (2 + cb) * E;
+    const uint32_t next = tile + gridDim.x;
+    if (next < P.n_tiles) issue(next, cb ^ 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+#pragma unroll
+    for (int ph = 0; ph < MAXPH; ++ph) {
+      if (ph >= P.n_phases) break;
+      const AdjPhase& D = P.ph[ph];
+      uint32_t sreg[LR];
+#pragma unroll
+      for (int k = 0; k < LR; ++k) sreg[k] = D.s_reg[k];
+#pragma unroll
+      for (int g = 0; g < GPT; ++g) {
+        const uint32_t q = (uint32_t)tid + (uint32_t)g * NT;
+        uint32_t sq = 0;
+#pragma unroll
+        for (int j = 0; j < M - LR; ++j)
+          if ((q >> j) & 1) sq ^= D.s_grp[j];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          a[r] = cp[sq ^ xsel<LR>(r, sreg)];
+          b[r] = cl[sq ^ xsel<LR>(r, sreg)];
+        }
+        adj_slot<R, LR, 0>(a, b, D.slot[0], acc[ph][0]);
+        if constexpr (LR > 1) adj_slot<R, LR, 1>(a, b, D.slot[1], acc[ph][1]);
+        if constexpr (LR > 2) adj_slot<R, LR, 2>(a, b, D.slot[2], acc[ph][2]);
+        if constexpr (LR > 3) adj_slot<R, LR, 3>(a, b, D.slot[3], acc[ph][3]);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+          if (P.store_psi) cp[sq ^ xsel<LR>(r, sreg)] = a[r];
+          cl[sq ^ xsel<LR>(r, sreg)] = b[r];
+        }
+      }
+      __syncthreads();
+    }
+    const uint32_t gb = base_of(tile) | g_t;
+    const float4* p4 = reinterpret_cast<const float4*>(cp);
+    const float4* l4 = reinterpret_cast<const float4*>(cl);
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+      if (P.store_psi) *reinterpret_cast<float4*>(psi + (gb | g_k(k))) = p4[slot(k)];
+      *reinterpret_cast<float4*>(lam + (gb | g_k(k))) = l4[slot(k)];
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+  // deterministic block reduction: lanes (xor tree), then warps in order
+  const int lane = tid & 31, warp = tid >> 5;
+  for (int j = tid; j < (NT + 31) / 32 * kAdjPartials; j += NT) (&red[0][0])[j] = 0.0;
+  __syncthreads();
+#pragma unroll
+  for (int p = 0; p < MAXPH; ++p)
+#pragma unroll
+    for (int k = 0; k < LR; ++k)
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        double v = (double)acc[p][k][s];
+#pragma unroll
+        for (int off = WS / 2; off; off >>= 1) v = __dadd_rn(v, __shfl_xor_sync(WMASK, v, off));
+        if (lane == 0) red[warp][(p * kAdjLR + k) * 2 + s] = v;
+      }
+  __syncthreads();
+  for (int j = tid; j < kAdjPartials; j += NT) {
+    double v = 0.0;
+    for (int w = 0; w < (NT + 31) / 32; ++w) v = __dadd_rn(v, red[w][j]);
+    partials[(size_t)blockIdx.x * kAdjPartials + j] = v;
+  }
+}
+
+// lam_x = d(x) psi_x with d(x) = sum_w c_w (-1)^popcount(x & z_w).
+constexpr int kHZWords = 64;
+struct HDiagParams {
+  uint32_t dim;
+  int32_t nz;
+  uint32_t z[kHZWords];
+  double c[kHZWords];
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_hdiag(const V2<R>* __restrict__ psi, V2<R>* __restrict__ lam,
+                                               const __grid_constant__ HDiagParams P) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.dim; i += stride) {
+    R d = 0;
+    for (int w = 0; w < P.nz; ++w) d += (__popc(i & P.z[w]) & 1) ? -(R)P.c[w] : (R)P.c[w];
+    const V2<R> v = psi[i];
+    lam[i] = mk<R>(d * v.x, d * v.y);
+  }
+}
+
+// per-block partial sums of Re <psi|lam> (fixed order)
+template <typename R>
+__global__ void __launch_bounds__(256) k_dot(const V2<R>* __restrict__ psi, const V2<R>* __restrict__ lam,
+                                             uint32_t dim, double* __restrict__ partials) {
+  __shared__ double red[8];
+  double acc = 0.0;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < dim; i += stride) {
+    const V2<R> p = psi[i], l = lam[i];
+    acc = __dadd_rn(acc, __dadd_rn(__dmul_rn((double)p.x, (double)l.x), __dmul_rn((double)p.y, (double)l.y)));
+  }
+#pragma unroll
+  for (int off = 16; off; off >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xffffffffu, acc, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v = __dadd_rn(v, red[w]);
+    partials[blockIdx.x] = v;
+  }
+}
+
+// ================================================================ host side
+static uint32_t adj_phys(bool c64, uint32_t i) { return c64 ? (i ^ ((i >> 3) & 0xEu)) : (i ^ ((i >> 3) & 7u)); }
+
+// One sweep: tile bits and, for each target (global index bit), its two steps.
+struct AdjTarget {
+  int bit;
+  uint8_t gen[2], has_u[2];
+  double u[2][8];
+};
+
+template <typename R, int M, int LR, int LT>
+static int launch_adj_t(mq_state* psi, mq_state* lam, const AdjParams& P, double* partials, uint32_t* grid_out) {
+  auto kern = k_adj<R, M, LR, LT>;
+  const size_t smem = 4 * sizeof(V2<R>) * (size_t(1) << M);
+  static int configured = -1, bps = 0;
+  if ((int)smem > configured) {
+    MQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
+    configured = (int)std::max<size_t>(smem, 48 * 1024);
+    MQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 1 << LT, smem));
+  }
+  const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(P.n_tiles, (uint64_t)psi->num_sms * std::max(1, bps)));
+  kern<<<grid, 1 << LT, smem, psi->stream>>>(reinterpret_cast<V2<R>*>(psi->cur_buf()),
+                                             reinterpret_cast<V2<R>*>(lam->cur_buf()), P, partials);
+  MQ_LAUNCHED("k_adj");
+  psi->launches += 1;
+  psi->sweeps += 2;
+  *grid_out = grid;
+  return MQ_OK;
+}
+
+template <typename R>
+static int dispatch_adj(mq_state* psi, mq_state* lam, const AdjParams& P, double* partials, uint32_t* grid) {
+  switch (P.m) {
+#define MQ_ADJ_CASE(MM)                                                              \
+    case MM: {                                                                       \
+      constexpr int LRT = sizeof(R) == 4 ? 4 : 3;                                    \
+      constexpr int L = (MM) < LRT ? (MM) : LRT;                                     \
+      constexpr int LT = ((MM) - L) < 7 ? ((MM) - L) : 7;                            \
+      return launch_adj_t<R, MM, L, LT>(psi, lam, P, partials, grid);                \
+    }
+    MQ_ADJ_CASE(1) MQ_ADJ_CASE(2) MQ_ADJ_CASE(3) MQ_ADJ_CASE(4) MQ_ADJ_CASE(5) MQ_ADJ_CASE(6)
+    MQ_ADJ_CASE(7) MQ_ADJ_CASE(8) MQ_ADJ_CASE(9) MQ_ADJ_CASE(10) MQ_ADJ_CASE(11)
+#undef MQ_ADJ_CASE
+    default: break;
+  }
+  return fail(MQ_EUNSUPPORTED, "adjoint tile size not instantiated");
+}
+
+// Run one sweep over `targets` (all within one tile); adds the gradient of
+// target t, step s to grads[t*2+s] (when grads is not null).
+static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarget>& targets,
+                         const std::vector<int>& tile_bits, bool store_psi, double* grads) {
+  const int n = psi->n;
+  const int m = (int)tile_bits.size();
+  const bool c64 = psi->dtype == MQ_C64;
+  const int lr = std::min(m, c64 ? 4 : 3);
+  const int maxph = (12 + (c64 ? 4 : 3) - 1) / (c64 ? 4 : 3);
+  if ((int)targets.size() > maxph * lr) return fail(MQ_EINVAL, "too many targets for one adjoint sweep");
+  AdjParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.n_tiles = (uint32_t)(uint64_t(1) << (n - m));
+  P.n = (uint8_t)n;
+  P.m = (uint8_t)m;
+  P.store_psi = store_psi ? 1 : 0;
+  for (int k = 0; k < m; ++k) P.tile_bit[k] = (uint8_t)tile_bits[k];
+  {
+    const int cb = c64 ? 1 : 0;
+    const int lt = std::min(7, m - lr);
+    const int first = cb + lt;
+    bool contig = true;
+    for (int b = first + 1; b < m; ++b)
+      if (tile_bits[b] != tile_bits[b - 1] + 1) contig = false;
+    P.hi_contig = (first < m && contig) ? 1 : 0;
+    P.hi_shift = (uint8_t)(first < m ? tile_bits[first] : 0);
+  }
+  // phases: targets in groups of lr, padded with the highest free tile bits
+  std::vector<int> local;
+  for (const auto& t : targets)
+    local.push_back((int)(std::find(tile_bits.begin(), tile_bits.end(), t.bit) - tile_bits.begin()));
+  std::vector<int> slot_target(kAdjMaxPhases * kAdjLR, -1);
+  int np = 0;
+  for (size_t i = 0; i < local.size(); i += lr, ++np) {
+    std::vector<int> regs(local.begin() + i, local.begin() + std::min(local.size(), i + lr));
+    for (int b = m - 1; (int)regs.size() < lr && b >= 0; --b)
+      if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
+    std::vector<int> sorted = regs;
+    std::sort(sorted.begin(), sorted.end());
+    AdjPhase& D = P.ph[np];
+    for (int k = 0; k < lr; ++k) D.s_reg[k] = adj_phys(c64, 1u << sorted[k]);
+    int j = 0;
+    for (int b = 0; b < m; ++b)
+      if (std::find(sorted.begin(), sorted.end(), b) == sorted.end()) D.s_grp[j++] = adj_phys(c64, 1u << b);
+    for (size_t t = i; t < std::min(local.size(), i + lr); ++t) {
+      const int k = (int)(std::find(sorted.begin(), sorted.end(), local[t]) - sorted.begin());
+      AdjSlot& S = D.slot[k];
+      for (int s = 0; s < 2; ++s) {
+        S.gen[s] = targets[t].gen[s];
+        S.has_u[s] = targets[t].has_u[s];
+        for (int e = 0; e < 8; ++e) {
+          S.ud[s][e] = targets[t].u[s][e];
+          S.uf[s][e] = (float)targets[t].u[s][e];
+        }
+      }
+      slot_target[np * kAdjLR + k] = (int)t;
+    }
+  }
+  P.n_phases = (uint8_t)np;
+  const uint32_t max_grid = (uint32_t)psi->num_sms * 32;
+  const size_t need = (size_t)max_grid * kAdjPartials * sizeof(double);
+  int rc = ensure_scratch(psi, need);
+  if (rc) return rc;
+  double* partials = reinterpret_cast<double*>(psi->scratch);
+  uint32_t grid = 0;
+  rc = c64 ? dispatch_adj<float>(psi, lam, P, partials, &grid) : dispatch_adj<double>(psi, lam, P, partials, &grid);
+  if (rc) return rc;
+  if (!grads) return MQ_OK;
+  std::vector<double> host((size_t)grid * kAdjPartials);
+  MQ_CUDA(cudaMemcpyAsync(host.data(), partials, host.size() * sizeof(double), cudaMemcpyDeviceToHost, psi->stream));
+  MQ_CUDA(cudaStreamSynchronize(psi->stream));
+  for (int sl = 0; sl < kAdjMaxPhases * kAdjLR; ++sl) {
+    const int t = slot_target[sl];
+    if (t < 0) continue;
+    for (int s = 0; s < 2; ++s) {
+      double v = 0.0;
+      for (uint32_t b = 0; b < grid; ++b) v += host[(size_t)b * kAdjPartials + sl * 2 + s];
+      grads[t * 2 + s] += v;
+    }
+  }
+  return MQ_OK;
+}
+
+// Tile groups: index bits split as the U(2) layer does, with tiles of at
+// most kAdjTileMax bits (psi and lam share shared memory).
+static int run_adj_layer(mq_state* psi, mq_state* lam, std::vector<AdjTarget> all, bool store_psi, double* grads,
+                         const std::vector<int>& order_of) {
+  const int n = psi->n;
+  const int tmax = std::min(kAdjTileMax, n);
+  const int pas = 4;
+  std::vector<std::pair<int, int>> groups;
+  if (n <= tmax) {
+    groups.push_back({0, n});
+  } else {
+    const int hi_cap = std::min(tmax - pas, kAdjMaxTargets);
+    const int n_hi = (n - tmax + hi_cap - 1) / hi_cap;
+    const int low = std::max(n - n_hi * hi_cap, std::min(tmax, (n + n_hi) / (n_hi + 1)));
+    groups.push_back({0, low});
+    int start = low;
+    const int rest = n - low;
+    for (int i = 0; i < n_hi; ++i) {
+      const int cnt = rest / n_hi + (i < rest % n_hi ? 1 : 0);
+      groups.push_back({start, cnt});
+      start += cnt;
+    }
+  }
+  std::vector<double> g(all.size() * 2, 0.0);
+  for (auto [start, cnt] : groups) {
+    std::vector<AdjTarget> tg;
+    std::vector<int> idx;
+    for (size_t i = 0; i < all.size(); ++i)
+      if (all[i].bit >= start && all[i].bit < start + cnt) { tg.push_back(all[i]); idx.push_back((int)i); }
+    if (tg.empty()) continue;
+    // split further if a group holds more targets than one sweep's phases
+    const size_t per = (size_t)((12 + (psi->dtype == MQ_C64 ? 4 : 3) - 1) / (psi->dtype == MQ_C64 ? 4 : 3)) *
+                       (size_t)std::min(psi->dtype == MQ_C64 ? 4 : 3, tmax);
+    for (size_t i0 = 0; i0 < tg.size(); i0 += per) {
+      std::vector<AdjTarget> part(tg.begin() + i0, tg.begin() + std::min(tg.size(), i0 + per));
+      std::vector<int> bits;
+      for (auto& t : part) bits.push_back(t.bit);
+      const int lowest = *std::min_element(bits.begin(), bits.end());
+      for (int b = 0; b < std::min(pas, lowest); ++b) bits.push_back(b);
+      std::sort(bits.begin(), bits.end());
+      bits.erase(std::unique(bits.begin(), bits.end()), bits.end());
+      for (int b = 0; (int)bits.size() < std::min(n, 10) && b < n; ++b)
+        if (std::find(bits.begin(), bits.end(), b) == bits.end()) bits.push_back(b);
+      std::sort(bits.begin(), bits.end());
+      if ((int)bits.size() > kAdjTileMax) return fail(MQ_EINVAL, "adjoint tile too large");
+      std::vector<double> pg(part.size() * 2, 0.0);
+      int rc = run_adj_sweep(psi, lam, part, bits, store_psi, grads ? pg.data() : nullptr);
+      if (rc) return rc;
+      for (size_t t = 0; t < part.size(); ++t) {
+        g[idx[i0 + t] * 2] += pg[t * 2];
+        g[idx[i0 + t] * 2 + 1] += pg[t * 2 + 1];
+      }
+    }
+  }
+  (void)order_of;
+  if (grads)
+    for (size_t i = 0; i < g.size(); ++i) grads[i] = g[i];
+  return MQ_OK;
+}
+
+int adjoint_sweep(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, const int32_t* gens,
+                  const double* mats, double* grads) {
+  const int n = psi->n;
+  std::vector<AdjTarget> all;
+  std::vector<bool> seen(n, false);
+  for (int i = 0; i < n_q; ++i) {
+    const int q = qubits[i];
+    if (q < 0 || q >= n) return fail(MQ_EINVAL, "Qubit index out of range");
+    if (seen[q]) return fail(MQ_EINVAL, "Duplicate qubit indices");
+    seen[q] = true;
+    AdjTarget t;
+    std::memset(&t, 0, sizeof(t));
+    t.bit = n - 1 - q;
+    for (int s = 0; s < 2; ++s) {
+      const int gen = gens[2 * i + s];
+      if (gen < GEN_NONE || gen > GEN_Z) return fail(MQ_EINVAL, "generator must be 0 (none), 1 (X), 2 (Y) or 3 (Z)");
+      t.gen[s] = (uint8_t)gen;
+      const double* u = mats + ((size_t)i * 2 + s) * 8;
+      bool ident = u[0] == 1.0 && u[1] == 0.0 && u[2] == 0.0 && u[3] == 0.0 && u[4] == 0.0 && u[5] == 0.0 &&
+                   u[6] == 1.0 && u[7] == 0.0;
+      t.has_u[s] = ident ? 0 : 1;
+      for (int e = 0; e < 8; ++e) t.u[s][e] = u[e];
+    }
+    all.push_back(t);
+  }
+  if (grads)
+    for (int i = 0; i < 2 * n_q; ++i) grads[i] = 0.0;
+  return run_adj_layer(psi, lam, all, true, grads, {});
+}
+
+int apply_hamiltonian(mq_state* psi, mq_state* lam, int n_z, const uint64_t* zmasks, const double* zcoef,
+                      const double* xcoef, double* energy) {
+  const int n = psi->n;
+  const uint64_t lim = psi->dim() - 1;
+  if (n_z > kHZWords) return fail(MQ_EUNSUPPORTED, "at most 64 Z words");
+  HDiagParams H;
+  std::memset(&H, 0, sizeof(H));
+  H.dim = (uint32_t)psi->dim();
+  H.nz = n_z;
+  for (int w = 0; w < n_z; ++w) {
+    if (zmasks[w] & ~lim) return fail(MQ_EINVAL, "Pauli mask outside the register");
+    H.z[w] = (uint32_t)zmasks[w];
+    H.c[w] = zcoef[w];
+  }
+  const uint32_t dim = (uint32_t)psi->dim();
+  const uint32_t grid = (uint32_t)std::min<uint64_t>((dim + 255) / 256, (uint64_t)psi->num_sms * 8);
+  if (psi->dtype == MQ_C64)
+    k_hdiag<float><<<grid, 256, 0, psi->stream>>>((const float2*)psi->cur_buf(), (float2*)lam->cur_buf(), H);
+  else
+    k_hdiag<double><<<grid, 256, 0, psi->stream>>>((const double2*)psi->cur_buf(), (double2*)lam->cur_buf(), H);
+  MQ_LAUNCHED("k_hdiag");
+  psi->launches += 1;
+  psi->sweeps += 1;
+  // X part through the tile sweeps (psi read-only)
+  std::vector<AdjTarget> xs;
+  for (int q = 0; q < n; ++q) {
+    if (!xcoef || xcoef[q] == 0.0) continue;
+    AdjTarget t;
+    std::memset(&t, 0, sizeof(t));
+    t.bit = n - 1 - q;
+    t.gen[0] = GEN_XADD;
+    t.u[0][0] = xcoef[q];
+    xs.push_back(t);
+  }
+  if (!xs.empty()) {
+    int rc = run_adj_layer(psi, lam, xs, false, nullptr, {});
+    if (rc) return rc;
+  }
+  if (!energy) return MQ_OK;
+  const uint32_t g2 = (uint32_t)psi->num_sms * 4;
+  int rc = ensure_scratch(psi, (size_t)g2 * sizeof(double));
+  if (rc) return rc;
+  double* partials = reinterpret_cast<double*>(psi->scratch);
+  if (psi->dtype == MQ_C64)
+    k_dot<float><<<g2, 256, 0, psi->stream>>>((const float2*)psi->cur_buf(), (const float2*)lam->cur_buf(), dim, partials);
+  else
+    k_dot<double><<<g2, 256, 0, psi->stream>>>((const double2*)psi->cur_buf(), (const double2*)lam->cur_buf(), dim, partials);
+  MQ_LAUNCHED("k_dot");
+  psi->launches += 1;
+  psi->sweeps += 1;
+  std::vector<double> host(g2);
+  MQ_CUDA(cudaMemcpyAsync(host.data(), partials, host.size() * sizeof(double), cudaMemcpyDeviceToHost, psi->stream));
+  MQ_CUDA(cudaStreamSynchronize(psi->stream));
+  double e = 0.0;
+  for (uint32_t b = 0; b < g2; ++b) e += host[b];
+  *energy = e;
+  return MQ_OK;
+}
+
+}  // namespace mq

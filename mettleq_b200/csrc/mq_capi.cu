@@ -183,6 +183,13 @@ int mq_state_set_stream(mq_state* h, void* stream) {
   return MQ_OK;
 }
 
+int mq_state_stream(const mq_state* h, void** out) {
+  MQ_CHECK_HANDLE(h);
+  if (!out) return fail(MQ_EINVAL, "null output");
+  *out = (void*)h->stream;
+  return MQ_OK;
+}
+
 int mq_state_reset(mq_state* h) {
   MQ_CHECK_HANDLE(h);
   DeviceGuard g(h->device);
@@ -441,6 +448,39 @@ int mq_expval_pauli(mq_state* h, int n_words, const uint64_t* xmask, const uint6
   if (!xmask || !zmask || !out) return fail(MQ_EINVAL, "null Pauli arrays");
   DeviceGuard g(h->device);
   return run_expval_pauli(h, n_words, xmask, zmask, ny, out);
+  MQ_TRY_END
+}
+
+static int check_pair(const mq_state* a, const mq_state* b) {
+  if (!a || !b) return fail(MQ_EINVAL, "null state handle");
+  if (a == b) return fail(MQ_EINVAL, "the two states must be different handles");
+  if (a->n != b->n || a->dtype != b->dtype || a->device != b->device)
+    return fail(MQ_EINVAL, "states differ in qubit count, dtype or device");
+  if (a->stream != b->stream) return fail(MQ_EINVAL, "both states must be bound to the same stream");
+  return MQ_OK;
+}
+
+int mq_apply_pauli_sum(mq_state* psi, mq_state* out, int n_z, const uint64_t* zmasks, const double* zcoef,
+                       const double* xcoef, double* energy) {
+  MQ_TRY_BEGIN
+  int rc = check_pair(psi, out);
+  if (rc) return rc;
+  if (n_z < 0 || (n_z > 0 && (!zmasks || !zcoef))) return fail(MQ_EINVAL, "invalid Z-word arrays");
+  DeviceGuard g(psi->device);
+  return apply_hamiltonian(psi, out, n_z, zmasks, zcoef, xcoef, energy);
+  MQ_TRY_END
+}
+
+int mq_adjoint_layer(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, const int32_t* gens,
+                     const double* mats, double* grads) {
+  MQ_TRY_BEGIN
+  int rc = check_pair(psi, lam);
+  if (rc) return rc;
+  if (n_q < 0) return fail(MQ_EINVAL, "negative qubit count");
+  if (n_q == 0) return MQ_OK;
+  if (!qubits || !gens || !mats) return fail(MQ_EINVAL, "null layer arrays");
+  DeviceGuard g(psi->device);
+  return adjoint_sweep(psi, lam, n_q, qubits, gens, mats, grads);
   MQ_TRY_END
 }
 

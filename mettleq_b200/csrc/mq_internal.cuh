@@ -145,6 +145,13 @@ int run_expval_pauli(mq_state* h, int n_words, const uint64_t* xmask, const uint
 int run_expval_pauli_static(mq_state* h, int n_words, const uint64_t* xmask, const uint64_t* zmask,
                             const int32_t* ny, double* out);
 
+// Adjoint method (mq_adjoint.cu): one backward layer on (psi, lam), and
+// lam = H psi for H = sum_w zcoef_w Z-word_w + sum_q xcoef_q X_q.
+int adjoint_sweep(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, const int32_t* gens,
+                  const double* mats, double* grads);
+int apply_hamiltonian(mq_state* psi, mq_state* lam, int n_z, const uint64_t* zmasks, const double* zcoef,
+                      const double* xcoef, double* energy);
+
 // GF(2) helpers (host)
 bool gf2_invert(int n, const uint32_t* cols, uint32_t* inv_cols);
 

@@ -137,6 +137,13 @@ class StateVector:
     def copy_from(self, other: "StateVector") -> None:
         N.check(self._lib.mq_state_copy(self._h, other._h))
 
+    @property
+    def stream(self) -> int:
+        """cudaStream_t (as an integer) the handle launches on."""
+        out = C.c_void_p()
+        N.check(self._lib.mq_state_stream(self._h, C.byref(out)))
+        return int(out.value or 0)
+
     def set_stream(self, stream: Optional[int]) -> None:
         N.check(self._lib.mq_state_set_stream(self._h, C.c_void_p(stream or 0)))
 
