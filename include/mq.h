@@ -156,13 +156,20 @@ int mq_expval_pauli(mq_state* h, int n_words, const uint64_t* xmask,
  * Re <psi|H|psi>. */
 int mq_apply_pauli_sum(mq_state* psi, mq_state* out, int n_z, const uint64_t* zmasks,
                        const double* zcoef, const double* xcoef, double* energy);
-/* One backward layer: for each listed qubit q_i and step s = 0, 1:
- * grads[2i+s] = Im <lam|G|psi> with G = gens[2i+s] (0 none, 1 X, 2 Y, 3 Z)
- * on q_i, then psi, lam <- mats[(2i+s)*8 ..] (2x2 complex128
- * [u00,u01,u10,u11]) on q_i.  For a gate exp(-i t G / 2) applied last in
- * the forward circuit, passing its inverse gives dE/dt. */
+/* One backward layer: for each listed qubit q_i, out[3i+0..2] = Im <lam|P|psi>
+ * for P = X, Y, Z on q_i, then psi, lam <- mats[8i ..] (2x2 complex128
+ * [u00,u01,u10,u11]) on q_i.  The 2x2s must commute (different qubits).
+ * For a qubit whose last forward gate was U = R_{K-1} ... R_0 with
+ * R_k = exp(-i t_k G_k / 2), pass U^dag: then dE/dt_k = a X + b Y + c Z
+ * read off out, with V G_k V^dag = aX + bY + cZ, V = R_{K-1} ... R_{k+1}.
+ * out == NULL: un-apply only. */
 int mq_adjoint_layer(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits,
-                     const int32_t* gens, const double* mats, double* grads);
+                     const double* mats, double* out);
+/* mq_adjoint_layer with out in DEVICE memory (3*n_q doubles), written on the
+ * stream without waiting for the GPU: a backward run of many layers reads
+ * its gradients back once. */
+int mq_adjoint_layer_async(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits,
+                           const double* mats, double* out_dev);
 
 /* mq_expval_pauli without any device allocation.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc or cudaFree

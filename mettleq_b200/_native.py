@@ -57,7 +57,8 @@ SIGNATURES = {
     "mq_expval_pauli": (_I, [_P, _I, _P, _P, _P, _P]),
     "mq_expval_pauli_static": (_I, [_P, _I, _P, _P, _P, _P]),
     "mq_apply_pauli_sum": (_I, [_P, _P, _I, _P, _P, _P, _P]),
-    "mq_adjoint_layer": (_I, [_P, _P, _I, _P, _P, _P, _P]),
+    "mq_adjoint_layer": (_I, [_P, _P, _I, _P, _P, _P]),
+    "mq_adjoint_layer_async": (_I, [_P, _P, _I, _P, _P, _P]),
 }
 
 

@@ -35,6 +35,9 @@ from .engine import StateVector
 from .workloads import cnot_ladder_rows
 
 GEN = {"RX": 1, "RY": 2, "RZ": 3}
+_PAULI = {"RX": np.array([[0, 1], [1, 0]], dtype=np.complex128),
+          "RY": np.array([[0, -1j], [1j, 0]], dtype=np.complex128),
+          "RZ": np.array([[1, 0], [0, -1]], dtype=np.complex128)}
 
 
 def _ptr(a: np.ndarray):
@@ -51,6 +54,29 @@ def rotation(name: str, t: float) -> np.ndarray:
     if name == "RZ":
         return np.array([[np.exp(-0.5j * t), 0], [0, np.exp(0.5j * t)]], dtype=np.complex128)
     raise ValueError(f"rotation must be RX, RY or RZ, not {name}")
+
+
+def rotations(name: str, t: np.ndarray) -> np.ndarray:
+    """exp(-i t G / 2) for an array of angles: (len(t), 4) [u00, u01, u10, u11]."""
+    t = np.asarray(t, dtype=np.float64)
+    c, s = np.cos(t / 2.0), np.sin(t / 2.0)
+    out = np.zeros((t.size, 4), dtype=np.complex128)
+    if name == "RX":
+        out[:, 0] = out[:, 3] = c
+        out[:, 1] = out[:, 2] = -1j * s
+    elif name == "RY":
+        out[:, 0] = out[:, 3] = c
+        out[:, 1], out[:, 2] = -s, s
+    elif name == "RZ":
+        out[:, 0], out[:, 3] = np.exp(-0.5j * t), np.exp(0.5j * t)
+    else:
+        raise ValueError(f"rotation must be RX, RY or RZ, not {name}")
+    return out
+
+
+def _dagger(m: np.ndarray) -> np.ndarray:
+    """Conjugate transpose of (k, 4) row-major 2x2 matrices."""
+    return np.conj(m[:, [0, 2, 1, 3]])
 
 
 @dataclass
@@ -96,13 +122,27 @@ class LayeredAnsatz:
 
     def layer_mats(self, p: np.ndarray) -> np.ndarray:
         """(n, 4) products R_last ... R_first of one layer's rotations."""
-        mats = np.empty((self.n, 4), dtype=np.complex128)
-        for q in range(self.n):
-            u = np.eye(2, dtype=np.complex128)
-            for k, name in enumerate(self.rots):
-                u = rotation(name, float(p[q, k])) @ u
-            mats[q] = u.reshape(4)
-        return mats
+        u = np.tile(np.eye(2, dtype=np.complex128).reshape(1, 2, 2), (self.n, 1, 1))
+        for k, name in enumerate(self.rots):
+            u = rotations(name, p[:, k]).reshape(self.n, 2, 2) @ u
+        return u.reshape(self.n, 4)
+
+    def generator_coefficients(self, p: np.ndarray) -> np.ndarray:
+        """(n, K, 3): for rotation k of every qubit, the real (a, b, c) with
+        V G_k V^dag = aX + bY + cZ, V = R_{K-1} ... R_{k+1} (the rotations
+        after it in the layer), so that dE/dt_k = a Im<lam|X|psi> +
+        b Im<lam|Y|psi> + c Im<lam|Z|psi> at the point after the layer's
+        rotations."""
+        K = len(self.rots)
+        out = np.zeros((self.n, K, 3), dtype=np.float64)
+        V = np.tile(np.eye(2, dtype=np.complex128).reshape(1, 2, 2), (self.n, 1, 1))
+        for k in reversed(range(K)):
+            G = _PAULI[self.rots[k]]
+            Gp = V @ G @ np.conj(np.transpose(V, (0, 2, 1)))
+            for j, P in enumerate((_PAULI["RX"], _PAULI["RY"], _PAULI["RZ"])):
+                out[:, k, j] = 0.5 * np.real(np.einsum("qab,ba->q", Gp, P))
+            V = V @ rotations(self.rots[k], p[:, k]).reshape(self.n, 2, 2)
+        return out
 
     def ops(self, params: np.ndarray) -> List[dict]:
         """The circuit as op dicts (for the oracle and the parameter-shift
@@ -181,37 +221,49 @@ class AdjointEngine:
     def backward(self, params: np.ndarray) -> np.ndarray:
         """dE/dparams by the adjoint sweeps; psi and lam must be the states
         that ``energy(params)`` left (psi = U|0>, lam = H psi).  Un-applies
-        the circuit from both states."""
+        the circuit from both states, one ``mq_adjoint_layer`` call per layer
+        (the per-qubit rotation product at once); the transition values of
+        every layer go to one device buffer, read back once."""
         A = self.ansatz
         params = np.asarray(params, dtype=np.float64).reshape(A.shape)
-        grad = np.zeros(A.shape, dtype=np.float64)
-        n, R = A.n, len(A.rots)
+        n, L = A.n, A.layers
         inv_rows, inv_c = _ladder_inverse_rows(n)
         qubits = np.arange(n, dtype=np.int32)
-        # the rotations of one qubit go in steps of two, last rotation first
-        for l in reversed(range(A.layers)):
+        dev = self._grad_buffer(L * 3 * n)
+        trans = np.zeros((L, n, 3), dtype=np.float64)
+        for i, l in enumerate(reversed(range(L))):
             if A.ladder:
                 self.psi.apply_xor_affine(inv_rows, inv_c)
                 self.lam.apply_xor_affine(inv_rows, inv_c)
-            ks = list(reversed(range(R)))
-            for s0 in range(0, R, 2):
-                pair = ks[s0:s0 + 2]
-                gens = np.zeros((n, 2), dtype=np.int32)
-                mats = np.zeros((n, 2, 4), dtype=np.complex128)
-                mats[:, :, 0] = mats[:, :, 3] = 1.0
-                for s, k in enumerate(pair):
-                    name = A.rots[k]
-                    gens[:, s] = GEN[name]
-                    for q in range(n):
-                        mats[q, s] = rotation(name, float(params[l, q, k])).conj().T.reshape(4)
-                g = np.zeros(2 * n, dtype=np.float64)
-                m = np.ascontiguousarray(mats).view(np.float64)
-                N.check(self._lib.mq_adjoint_layer(self.psi.handle, self.lam.handle, n, _ptr(qubits),
-                                                   _ptr(gens), _ptr(m), _ptr(g)))
-                g = g.reshape(n, 2)
-                for s, k in enumerate(pair):
-                    grad[l, :, k] = g[:, s]
+            m = np.ascontiguousarray(_dagger(A.layer_mats(params[l]))).view(np.float64)
+            if dev is not None:
+                N.check(self._lib.mq_adjoint_layer_async(self.psi.handle, self.lam.handle, n, _ptr(qubits), _ptr(m),
+                                                         C.c_void_p(dev.data_ptr() + i * 3 * n * 8)))
+            else:
+                t = np.zeros(3 * n, dtype=np.float64)
+                N.check(self._lib.mq_adjoint_layer(self.psi.handle, self.lam.handle, n, _ptr(qubits), _ptr(m),
+                                                   _ptr(t)))
+                trans[i] = t.reshape(n, 3)
+        if dev is not None:
+            self.psi.synchronize()
+            trans = dev[: L * 3 * n].cpu().numpy().reshape(L, n, 3)
+        grad = np.zeros(A.shape, dtype=np.float64)
+        for i, l in enumerate(reversed(range(L))):
+            coef = A.generator_coefficients(params[l])          # (n, K, 3)
+            grad[l] = np.einsum("qkp,qp->qk", coef, trans[i])
         return grad
+
+    def _grad_buffer(self, count: int):
+        """Device buffer of ``count`` doubles (torch plumbing), or None."""
+        try:
+            import torch
+        except ImportError:  # pragma: no cover
+            return None
+        buf = getattr(self, "_gbuf", None)
+        if buf is None or buf.numel() < count:
+            buf = torch.empty(count, dtype=torch.float64, device=f"cuda:{self.psi.device}")
+            self._gbuf = buf
+        return buf
 
 
 def parameter_shift_grad(energy_fn, params: np.ndarray) -> np.ndarray:

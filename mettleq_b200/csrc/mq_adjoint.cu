@@ -15,8 +15,13 @@
 // applied to both psi and lam leaves <lam|G_q|psi> unchanged when it acts on
 // other qubits, so a whole layer is handled by tile sweeps over index-bit
 // groups (as the U(2) layer): k_adj streams tiles of psi and lam through
-// shared memory together and, for every target bit, accumulates the
-// gradient of each generator just before un-applying its gate.
+// shared memory together and, for every target qubit, accumulates the three
+// transition values Im <lam|P_q|psi> (P = X, Y, Z) and then un-applies the
+// qubit's whole rotation product U_q in one 2x2 step.  The gradient of any
+// rotation inside U_q is a real combination of the three: for
+// U_q = R_{K-1} ... R_0 and R_k = exp(-i t G / 2), taken at the point after
+// U_q, dE/dt_k = Im <lam| V G V^dag |psi> with V = R_{K-1} ... R_{k+1}, and
+// V G V^dag = a X + b Y + c Z (the host forms a, b, c).
 //
 //   k_hdiag: lam = D psi for the Z-word part of H (one pass)
 //   k_adj (build mode): lam += sum_q c_q X_q psi (tile sweeps)
@@ -30,21 +35,21 @@
 
 namespace mq {
 
-enum : uint8_t { GEN_NONE = 0, GEN_X = 1, GEN_Y = 2, GEN_Z = 3, GEN_XADD = 4 };
+enum : uint8_t { SLOT_NONE = 0, SLOT_MEASURE = 1, SLOT_XADD = 2 };
 
 constexpr int kAdjLR = 4;           // register bits per phase, complex64 (complex128: 3)
 constexpr int kAdjMaxPhases = 4;    // up to 12 target bits per sweep
 constexpr int kAdjTileMax = 11;     // psi and lam tiles, double-buffered: 4 * 2^11 * 8 B (complex64)
 constexpr int kAdjSlots = kAdjMaxPhases * kAdjLR;
-constexpr int kAdjPartials = 2 * kAdjSlots;  // per block: one double per (slot, step)
+constexpr int kAdjPartials = 3 * kAdjSlots;  // per block: Im <lam|X,Y,Z|psi> per slot
 constexpr int kAdjMaxTargets = 12;
 
 struct AdjSlot {
-  uint8_t gen[2];      // generator whose gradient is taken before step s
-  uint8_t has_u[2];    // step s un-applies a 2x2 gate
-  uint8_t pad[4];
-  alignas(16) float uf[2][8];
-  alignas(16) double ud[2][8];  // GEN_XADD: ud[s][0] = coefficient
+  uint8_t mode;        // SLOT_MEASURE: transition values, then un-apply u
+  uint8_t has_u;       // u is not the identity
+  uint8_t pad[6];
+  alignas(16) float uf[8];
+  alignas(16) double ud[8];  // SLOT_XADD: ud[0] = coefficient of X_q
 };
 
 struct AdjPhase {
@@ -62,9 +67,9 @@ struct AdjParams {
 };
 
 template <typename R>
-__device__ __forceinline__ V2<R> slot_u(const AdjSlot& S, int s, int j) {
-  if constexpr (sizeof(R) == 4) return make_float2(S.uf[s][2 * j], S.uf[s][2 * j + 1]);
-  else return make_double2(S.ud[s][2 * j], S.ud[s][2 * j + 1]);
+__device__ __forceinline__ V2<R> slot_u(const AdjSlot& S, int j) {
+  if constexpr (sizeof(R) == 4) return make_float2(S.uf[2 * j], S.uf[2 * j + 1]);
+  else return make_double2(S.ud[2 * j], S.ud[2 * j + 1]);
 }
 
 template <typename T>
@@ -75,43 +80,28 @@ __device__ __forceinline__ T cmac(T u0, T x0, T u1, T x1) {
   return r;
 }
 
-// Gradient partial of generator `gen` on register bit K, then the step's gate
-// on both register sets.
+// Register bit K: transition values Im <lam|P|psi> for P = X, Y, Z over the
+// thread's pairs (SLOT_MEASURE), then the 2x2 un-apply on both register
+// sets; SLOT_XADD adds c X_q psi to lam instead.
 template <typename R, int LR, int K>
 __device__ __forceinline__ void adj_slot(V2<R> (&a)[1 << LR], V2<R> (&b)[1 << LR], const AdjSlot& S,
-                                         R (&acc)[2]) {
+                                         R (&acc)[3]) {
   using T = V2<R>;
+  if (S.mode == SLOT_MEASURE) {
+    R gx = 0, gy = 0, gz = 0;
 #pragma unroll
-  for (int s = 0; s < 2; ++s) {
-    const int gen = S.gen[s];
-    if (gen != GEN_NONE && gen != GEN_XADD) {
-      R g = 0;
-#pragma unroll
-      for (int r = 0; r < (1 << LR); ++r) {
-        if (r & (1 << K)) continue;
-        const T x0 = a[r], x1 = a[r | (1 << K)], l0 = b[r], l1 = b[r | (1 << K)];
-        if (gen == GEN_Z) {
-          g += (l0.x * x0.y - l0.y * x0.x) - (l1.x * x1.y - l1.y * x1.x);
-        } else if (gen == GEN_Y) {
-          g += (l1.x * x0.x + l1.y * x0.y) - (l0.x * x1.x + l0.y * x1.y);
-        } else {
-          g += (l0.x * x1.y - l0.y * x1.x) + (l1.x * x0.y - l1.y * x0.x);
-        }
-      }
-      acc[s] += g;
+    for (int r = 0; r < (1 << LR); ++r) {
+      if (r & (1 << K)) continue;
+      const T x0 = a[r], x1 = a[r | (1 << K)], l0 = b[r], l1 = b[r | (1 << K)];
+      gz += (l0.x * x0.y - l0.y * x0.x) - (l1.x * x1.y - l1.y * x1.x);
+      gy += (l1.x * x0.x + l1.y * x0.y) - (l0.x * x1.x + l0.y * x1.y);
+      gx += (l0.x * x1.y - l0.y * x1.x) + (l1.x * x0.y - l1.y * x0.x);
     }
-    if (gen == GEN_XADD) {
-      const R c = (R)S.ud[s][0];
-#pragma unroll
-      for (int r = 0; r < (1 << LR); ++r) {
-        if (r & (1 << K)) continue;
-        const T x0 = a[r], x1 = a[r | (1 << K)];
-        b[r].x += c * x1.x; b[r].y += c * x1.y;
-        b[r | (1 << K)].x += c * x0.x; b[r | (1 << K)].y += c * x0.y;
-      }
-    }
-    if (S.has_u[s]) {
-      const T u00 = slot_u<R>(S, s, 0), u01 = slot_u<R>(S, s, 1), u10 = slot_u<R>(S, s, 2), u11 = slot_u<R>(S, s, 3);
+    acc[0] += gx;
+    acc[1] += gy;
+    acc[2] += gz;
+    if (S.has_u) {
+      const T u00 = slot_u<R>(S, 0), u01 = slot_u<R>(S, 1), u10 = slot_u<R>(S, 2), u11 = slot_u<R>(S, 3);
 #pragma unroll
       for (int r = 0; r < (1 << LR); ++r) {
         if (r & (1 << K)) continue;
@@ -123,6 +113,15 @@ __device__ __forceinline__ void adj_slot(V2<R> (&a)[1 << LR], V2<R> (&b)[1 << LR
         b[r] = cmac(u00, y0, u01, y1);
         b[r1] = cmac(u10, y0, u11, y1);
       }
+    }
+  } else if (S.mode == SLOT_XADD) {
+    const R c = (R)S.ud[0];
+#pragma unroll
+    for (int r = 0; r < (1 << LR); ++r) {
+      if (r & (1 << K)) continue;
+      const T x0 = a[r], x1 = a[r | (1 << K)];
+      b[r].x += c * x1.x; b[r].y += c * x1.y;
+      b[r | (1 << K)].x += c * x0.x; b[r | (1 << K)].y += c * x0.y;
     }
   }
 }
@@ -197,11 +196,11 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
   // (a few dozen terms each); blocks reduce them in double
   constexpr int MAXPH = (12 + LR - 1) / LR < kAdjMaxPhases ? (12 + LR - 1) / LR : kAdjMaxPhases;
   static_assert(MAXPH <= kAdjMaxPhases, "too many phases");
-  R acc[MAXPH][LR][2];
+  R acc[MAXPH][LR][3];
 #pragma unroll
   for (int p = 0; p < MAXPH; ++p)
 #pragma unroll
-    for (int k = 0; k < LR; ++k) acc[p][k][0] = acc[p][k][1] = 0;
+    for (int k = 0; k < LR; ++k) acc[p][k][0] = acc[p][k][1] = acc[p][k][2] = 0;
 
   uint32_t tile = blockIdx.x;
   if (tile < P.n_tiles) issue(tile, 0);
@@ -267,11 +266,11 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
 #pragma unroll
     for (int k = 0; k < LR; ++k)
 #pragma unroll
-      for (int s = 0; s < 2; ++s) {
+      for (int s = 0; s < 3; ++s) {
         double v = (double)acc[p][k][s];
 #pragma unroll
         for (int off = WS / 2; off; off >>= 1) v = __dadd_rn(v, __shfl_xor_sync(WMASK, v, off));
-        if (lane == 0) red[warp][(p * kAdjLR + k) * 2 + s] = v;
+        if (lane == 0) red[warp][(p * kAdjLR + k) * 3 + s] = v;
       }
   __syncthreads();
   for (int j = tid; j < kAdjPartials; j += NT) {
@@ -324,14 +323,30 @@ __global__ void __launch_bounds__(256) k_dot(const V2<R>* __restrict__ psi, cons
   }
 }
 
+// out[index[j/3]*3 + j%3] = sum over blocks b (in order) of partials[b][j]
+// for every (slot, Pauli) j whose slot carries a target.
+struct AdjCollect {
+  int32_t index[kAdjSlots];
+};
+__global__ void k_adj_collect(const double* __restrict__ partials, uint32_t nblocks, const __grid_constant__ AdjCollect C,
+                              double* __restrict__ out) {
+  const int j = threadIdx.x;
+  if (j >= kAdjPartials) return;
+  const int t = C.index[j / 3];
+  if (t < 0) return;
+  double v = 0.0;
+  for (uint32_t b = 0; b < nblocks; ++b) v = __dadd_rn(v, partials[(size_t)b * kAdjPartials + j]);
+  out[t * 3 + j % 3] = v;
+}
+
 // ================================================================ host side
 static uint32_t adj_phys(bool c64, uint32_t i) { return c64 ? (i ^ ((i >> 3) & 0xEu)) : (i ^ ((i >> 3) & 7u)); }
 
 // One sweep: tile bits and, for each target (global index bit), its two steps.
 struct AdjTarget {
   int bit;
-  uint8_t gen[2], has_u[2];
-  double u[2][8];
+  uint8_t mode, has_u;
+  double u[8];
 };
 
 template <typename R, int M, int LR, int LT>
@@ -372,10 +387,12 @@ static int dispatch_adj(mq_state* psi, mq_state* lam, const AdjParams& P, double
   return fail(MQ_EUNSUPPORTED, "adjoint tile size not instantiated");
 }
 
-// Run one sweep over `targets` (all within one tile); adds the gradient of
-// target t, step s to grads[t*2+s] (when grads is not null).
+// Run one sweep over `targets` (all within one tile).  With grads_dev, the
+// gradient of target t, step s is written to grads_dev[index[t]*2+s]
+// (device memory) on the stream.
 static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarget>& targets,
-                         const std::vector<int>& tile_bits, bool store_psi, double* grads) {
+                         const std::vector<int>& tile_bits, bool store_psi, const std::vector<int>& index,
+                         double* grads_dev) {
   const int n = psi->n;
   const int m = (int)tile_bits.size();
   const bool c64 = psi->dtype == MQ_C64;
@@ -419,13 +436,11 @@ static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
     for (size_t t = i; t < std::min(local.size(), i + lr); ++t) {
       const int k = (int)(std::find(sorted.begin(), sorted.end(), local[t]) - sorted.begin());
       AdjSlot& S = D.slot[k];
-      for (int s = 0; s < 2; ++s) {
-        S.gen[s] = targets[t].gen[s];
-        S.has_u[s] = targets[t].has_u[s];
-        for (int e = 0; e < 8; ++e) {
-          S.ud[s][e] = targets[t].u[s][e];
-          S.uf[s][e] = (float)targets[t].u[s][e];
-        }
+      S.mode = targets[t].mode;
+      S.has_u = targets[t].has_u;
+      for (int e = 0; e < 8; ++e) {
+        S.ud[e] = targets[t].u[e];
+        S.uf[e] = (float)targets[t].u[e];
       }
       slot_target[np * kAdjLR + k] = (int)t;
     }
@@ -439,29 +454,23 @@ static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
   uint32_t grid = 0;
   rc = c64 ? dispatch_adj<float>(psi, lam, P, partials, &grid) : dispatch_adj<double>(psi, lam, P, partials, &grid);
   if (rc) return rc;
-  if (!grads) return MQ_OK;
-  std::vector<double> host((size_t)grid * kAdjPartials);
-  MQ_CUDA(cudaMemcpyAsync(host.data(), partials, host.size() * sizeof(double), cudaMemcpyDeviceToHost, psi->stream));
-  MQ_CUDA(cudaStreamSynchronize(psi->stream));
-  for (int sl = 0; sl < kAdjMaxPhases * kAdjLR; ++sl) {
-    const int t = slot_target[sl];
-    if (t < 0) continue;
-    for (int s = 0; s < 2; ++s) {
-      double v = 0.0;
-      for (uint32_t b = 0; b < grid; ++b) v += host[(size_t)b * kAdjPartials + sl * 2 + s];
-      grads[t * 2 + s] += v;
-    }
-  }
+  if (!grads_dev) return MQ_OK;
+  AdjCollect C;
+  for (int sl = 0; sl < kAdjSlots; ++sl) C.index[sl] = slot_target[sl] < 0 ? -1 : index[slot_target[sl]];
+  k_adj_collect<<<1, kAdjPartials, 0, psi->stream>>>(partials, grid, C, grads_dev);
+  MQ_LAUNCHED("k_adj_collect");
+  psi->launches += 1;
   return MQ_OK;
 }
 
 // Tile groups: index bits split as the U(2) layer does, with tiles of at
 // most kAdjTileMax bits (psi and lam share shared memory).
-static int run_adj_layer(mq_state* psi, mq_state* lam, std::vector<AdjTarget> all, bool store_psi, double* grads,
-                         const std::vector<int>& order_of) {
+static int run_adj_layer(mq_state* psi, mq_state* lam, const std::vector<AdjTarget>& all, bool store_psi,
+                         double* grads_dev) {
   const int n = psi->n;
   const int tmax = std::min(kAdjTileMax, n);
   const int pas = 4;
+  const int lrt = psi->dtype == MQ_C64 ? 4 : 3;
   std::vector<std::pair<int, int>> groups;
   if (n <= tmax) {
     groups.push_back({0, n});
@@ -478,18 +487,17 @@ static int run_adj_layer(mq_state* psi, mq_state* lam, std::vector<AdjTarget> al
       start += cnt;
     }
   }
-  std::vector<double> g(all.size() * 2, 0.0);
+  const size_t per = (size_t)((12 + lrt - 1) / lrt) * (size_t)std::min(lrt, tmax);
   for (auto [start, cnt] : groups) {
     std::vector<AdjTarget> tg;
     std::vector<int> idx;
     for (size_t i = 0; i < all.size(); ++i)
       if (all[i].bit >= start && all[i].bit < start + cnt) { tg.push_back(all[i]); idx.push_back((int)i); }
-    if (tg.empty()) continue;
     // split further if a group holds more targets than one sweep's phases
-    const size_t per = (size_t)((12 + (psi->dtype == MQ_C64 ? 4 : 3) - 1) / (psi->dtype == MQ_C64 ? 4 : 3)) *
-                       (size_t)std::min(psi->dtype == MQ_C64 ? 4 : 3, tmax);
     for (size_t i0 = 0; i0 < tg.size(); i0 += per) {
-      std::vector<AdjTarget> part(tg.begin() + i0, tg.begin() + std::min(tg.size(), i0 + per));
+      const size_t i1 = std::min(tg.size(), i0 + per);
+      std::vector<AdjTarget> part(tg.begin() + i0, tg.begin() + i1);
+      std::vector<int> pidx(idx.begin() + i0, idx.begin() + i1);
       std::vector<int> bits;
       for (auto& t : part) bits.push_back(t.bit);
       const int lowest = *std::min_element(bits.begin(), bits.end());
@@ -500,23 +508,15 @@ static int run_adj_layer(mq_state* psi, mq_state* lam, std::vector<AdjTarget> al
         if (std::find(bits.begin(), bits.end(), b) == bits.end()) bits.push_back(b);
       std::sort(bits.begin(), bits.end());
       if ((int)bits.size() > kAdjTileMax) return fail(MQ_EINVAL, "adjoint tile too large");
-      std::vector<double> pg(part.size() * 2, 0.0);
-      int rc = run_adj_sweep(psi, lam, part, bits, store_psi, grads ? pg.data() : nullptr);
+      int rc = run_adj_sweep(psi, lam, part, bits, store_psi, pidx, grads_dev);
       if (rc) return rc;
-      for (size_t t = 0; t < part.size(); ++t) {
-        g[idx[i0 + t] * 2] += pg[t * 2];
-        g[idx[i0 + t] * 2 + 1] += pg[t * 2 + 1];
-      }
     }
   }
-  (void)order_of;
-  if (grads)
-    for (size_t i = 0; i < g.size(); ++i) grads[i] = g[i];
   return MQ_OK;
 }
 
-int adjoint_sweep(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, const int32_t* gens,
-                  const double* mats, double* grads) {
+int adjoint_sweep(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, const double* mats, double* out,
+                  bool out_on_device) {
   const int n = psi->n;
   std::vector<AdjTarget> all;
   std::vector<bool> seen(n, false);
@@ -528,21 +528,29 @@ int adjoint_sweep(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, 
     AdjTarget t;
     std::memset(&t, 0, sizeof(t));
     t.bit = n - 1 - q;
-    for (int s = 0; s < 2; ++s) {
-      const int gen = gens[2 * i + s];
-      if (gen < GEN_NONE || gen > GEN_Z) return fail(MQ_EINVAL, "generator must be 0 (none), 1 (X), 2 (Y) or 3 (Z)");
-      t.gen[s] = (uint8_t)gen;
-      const double* u = mats + ((size_t)i * 2 + s) * 8;
-      bool ident = u[0] == 1.0 && u[1] == 0.0 && u[2] == 0.0 && u[3] == 0.0 && u[4] == 0.0 && u[5] == 0.0 &&
-                   u[6] == 1.0 && u[7] == 0.0;
-      t.has_u[s] = ident ? 0 : 1;
-      for (int e = 0; e < 8; ++e) t.u[s][e] = u[e];
-    }
+    t.mode = SLOT_MEASURE;
+    const double* u = mats + (size_t)i * 8;
+    const bool ident = u[0] == 1.0 && u[1] == 0.0 && u[2] == 0.0 && u[3] == 0.0 && u[4] == 0.0 && u[5] == 0.0 &&
+                       u[6] == 1.0 && u[7] == 0.0;
+    t.has_u = ident ? 0 : 1;
+    for (int e = 0; e < 8; ++e) t.u[e] = u[e];
     all.push_back(t);
   }
-  if (grads)
-    for (int i = 0; i < 2 * n_q; ++i) grads[i] = 0.0;
-  return run_adj_layer(psi, lam, all, true, grads, {});
+  double* grads = out;
+  const bool grads_on_device = out_on_device;
+  // scratch: per-block partials, then (host output) the layer's gradients
+  const size_t part_bytes = (size_t)psi->num_sms * 32 * kAdjPartials * sizeof(double);
+  int rc = ensure_scratch(psi, part_bytes + (size_t)3 * n_q * sizeof(double) + 256);
+  if (rc) return rc;
+  double* dev = grads_on_device ? grads : (grads ? reinterpret_cast<double*>(static_cast<char*>(psi->scratch) + part_bytes) : nullptr);
+  if (dev) MQ_CUDA(cudaMemsetAsync(dev, 0, (size_t)3 * n_q * sizeof(double), psi->stream));
+  rc = run_adj_layer(psi, lam, all, true, dev);
+  if (rc) return rc;
+  if (grads && !grads_on_device) {
+    MQ_CUDA(cudaMemcpyAsync(grads, dev, (size_t)3 * n_q * sizeof(double), cudaMemcpyDeviceToHost, psi->stream));
+    MQ_CUDA(cudaStreamSynchronize(psi->stream));
+  }
+  return MQ_OK;
 }
 
 int apply_hamiltonian(mq_state* psi, mq_state* lam, int n_z, const uint64_t* zmasks, const double* zcoef,
@@ -575,12 +583,12 @@ int apply_hamiltonian(mq_state* psi, mq_state* lam, int n_z, const uint64_t* zma
     AdjTarget t;
     std::memset(&t, 0, sizeof(t));
     t.bit = n - 1 - q;
-    t.gen[0] = GEN_XADD;
-    t.u[0][0] = xcoef[q];
+    t.mode = SLOT_XADD;
+    t.u[0] = xcoef[q];
     xs.push_back(t);
   }
   if (!xs.empty()) {
-    int rc = run_adj_layer(psi, lam, xs, false, nullptr, {});
+    int rc = run_adj_layer(psi, lam, xs, false, nullptr);
     if (rc) return rc;
   }
   if (!energy) return MQ_OK;

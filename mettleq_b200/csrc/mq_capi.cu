@@ -471,16 +471,29 @@ int mq_apply_pauli_sum(mq_state* psi, mq_state* out, int n_z, const uint64_t* zm
   MQ_TRY_END
 }
 
-int mq_adjoint_layer(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, const int32_t* gens,
-                     const double* mats, double* grads) {
+int mq_adjoint_layer(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, const double* mats,
+                     double* out) {
   MQ_TRY_BEGIN
   int rc = check_pair(psi, lam);
   if (rc) return rc;
   if (n_q < 0) return fail(MQ_EINVAL, "negative qubit count");
   if (n_q == 0) return MQ_OK;
-  if (!qubits || !gens || !mats) return fail(MQ_EINVAL, "null layer arrays");
+  if (!qubits || !mats) return fail(MQ_EINVAL, "null layer arrays");
   DeviceGuard g(psi->device);
-  return adjoint_sweep(psi, lam, n_q, qubits, gens, mats, grads);
+  return adjoint_sweep(psi, lam, n_q, qubits, mats, out, false);
+  MQ_TRY_END
+}
+
+int mq_adjoint_layer_async(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, const double* mats,
+                           double* out_dev) {
+  MQ_TRY_BEGIN
+  int rc = check_pair(psi, lam);
+  if (rc) return rc;
+  if (n_q < 0) return fail(MQ_EINVAL, "negative qubit count");
+  if (n_q == 0) return MQ_OK;
+  if (!qubits || !mats || !out_dev) return fail(MQ_EINVAL, "null layer arrays");
+  DeviceGuard g(psi->device);
+  return adjoint_sweep(psi, lam, n_q, qubits, mats, out_dev, true);
   MQ_TRY_END
 }
 

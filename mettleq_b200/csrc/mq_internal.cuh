@@ -127,11 +127,27 @@ struct DiagWindows {
 };
 int plan_diag_windows(mq_state* h, int n_terms, const int32_t* kinds, const int32_t* wires, const double* params,
                       int max_entries, DiagWindows& out);
+// A diagonal factored for a 4-bit register phase (plan_diag_register):
+// window tables (win, evaluated at the register group's base) followed, at
+// entry t_off, by T[c][r] (16 << nc entries) indexed by the register bits r
+// and the cross bits c = bits cbit[0..nc) of the index.
+struct DiagRegister {
+  DiagWindows win;
+  int nc = 0;
+  int cbit[3] = {};
+  int t_off = 0;
+};
+int plan_diag_register(mq_state* h, int n_terms, const int32_t* kinds, const int32_t* wires, const double* params,
+                       const int* rbits, int max_entries, DiagRegister& out);
 // Fused layer: U(2) on every active qubit, then the diagonal terms, then the
 // GF(2) permutation out[y] = in[A y ^ c] (cols = A e_j; null = none)
 // (mq_tile.cu).
+// mats == NULL with mats_dev: the U(2) matrices are read from device memory
+// (n rows of 8 doubles) when the sweeps run, so a captured graph of the
+// layer stays valid when the matrices change.
 int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_terms, const int32_t* kinds,
-                 const int32_t* wires, const double* params, const uint32_t* cols, uint32_t c);
+                 const int32_t* wires, const double* params, const uint32_t* cols, uint32_t c,
+                 const double* mats_dev = nullptr);
 // GF(2) affine permutation, out-of-place into the alternate buffer (mq_perm.cu).
 // cols[j] = A e_j (index-bit columns of the source map), c = flip constant.
 int launch_affine_cols(mq_state* h, const uint32_t* cols, uint32_t c);
@@ -147,8 +163,8 @@ int run_expval_pauli_static(mq_state* h, int n_words, const uint64_t* xmask, con
 
 // Adjoint method (mq_adjoint.cu): one backward layer on (psi, lam), and
 // lam = H psi for H = sum_w zcoef_w Z-word_w + sum_q xcoef_q X_q.
-int adjoint_sweep(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, const int32_t* gens,
-                  const double* mats, double* grads);
+int adjoint_sweep(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, const double* mats, double* out,
+                  bool out_on_device);
 int apply_hamiltonian(mq_state* psi, mq_state* lam, int n_z, const uint64_t* zmasks, const double* zcoef,
                       const double* xcoef, double* energy);
 

@@ -188,3 +188,22 @@ def test_pauli_sum_energy_and_lambda():
         out += c * o2.state
     assert abs(e - ref_e) < 1e-12
     assert np.max(np.abs(lam - out)) < 1e-12
+
+
+@pytest.mark.gpu
+def test_host_and_device_gradient_readback_agree(monkeypatch):
+    """mq_adjoint_layer (host gradients, one wait per layer) and
+    mq_adjoint_layer_async (device gradients, one read at the end) give the
+    same bits."""
+    from mettleq_b200.adjoint import AdjointEngine
+    A = LayeredAnsatz(14, 3, ("RX", "RY", "RZ"))
+    H = PauliSum.ising_chain(14, 0.8, -0.3)
+    p = np.random.default_rng(8).uniform(-math.pi, math.pi, A.shape)
+    eng = AdjointEngine(A, H, dtype="complex64")
+    try:
+        _, g_dev = eng.energy_and_grad(p)
+        monkeypatch.setattr(eng, "_grad_buffer", lambda count: None)
+        _, g_host = eng.energy_and_grad(p)
+    finally:
+        eng.close()
+    assert np.array_equal(g_dev, g_host)
