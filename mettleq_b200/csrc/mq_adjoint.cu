@@ -28,6 +28,7 @@
 //   k_dot:   E = Re <psi|lam> (one pass)
 //   k_adj (backward mode): gradients + un-apply, per layer
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -369,14 +370,22 @@ static int launch_adj_t(mq_state* psi, mq_state* lam, const AdjParams& P, double
   return MQ_OK;
 }
 
-template <typename R>
-static int dispatch_adj(mq_state* psi, mq_state* lam, const AdjParams& P, double* partials, uint32_t* grid) {
+// Register bits per phase: 3 (more threads per tile and fewer registers per
+// thread than 4, measured faster); complex64 takes 4 with MQ_ADJ_LR=4.
+static int adj_lr(int dtype) {
+  if (dtype != MQ_C64) return 3;
+  const char* v = std::getenv("MQ_ADJ_LR");
+  return (v && std::atoi(v) == 4) ? 4 : 3;
+}
+
+template <typename R, int LRT>
+static int dispatch_adj_lr(mq_state* psi, mq_state* lam, const AdjParams& P, double* partials, uint32_t* grid) {
   switch (P.m) {
 #define MQ_ADJ_CASE(MM)                                                              \
     case MM: {                                                                       \
-      constexpr int LRT = sizeof(R) == 4 ? 4 : 3;                                    \
       constexpr int L = (MM) < LRT ? (MM) : LRT;                                     \
-      constexpr int LT = ((MM) - L) < 7 ? ((MM) - L) : 7;                            \
+      constexpr int LTMAX = LRT == 3 ? 8 : 7;                                        \
+      constexpr int LT = ((MM) - L) < LTMAX ? ((MM) - L) : LTMAX;                    \
       return launch_adj_t<R, MM, L, LT>(psi, lam, P, partials, grid);                \
     }
     MQ_ADJ_CASE(1) MQ_ADJ_CASE(2) MQ_ADJ_CASE(3) MQ_ADJ_CASE(4) MQ_ADJ_CASE(5) MQ_ADJ_CASE(6)
@@ -385,6 +394,15 @@ static int dispatch_adj(mq_state* psi, mq_state* lam, const AdjParams& P, double
     default: break;
   }
   return fail(MQ_EUNSUPPORTED, "adjoint tile size not instantiated");
+}
+
+template <typename R>
+static int dispatch_adj(mq_state* psi, mq_state* lam, const AdjParams& P, double* partials, uint32_t* grid) {
+  if constexpr (sizeof(R) == 4) {
+    if (adj_lr(MQ_C64) == 3) return dispatch_adj_lr<R, 3>(psi, lam, P, partials, grid);
+    return dispatch_adj_lr<R, 4>(psi, lam, P, partials, grid);
+  }
+  return dispatch_adj_lr<R, 3>(psi, lam, P, partials, grid);
 }
 
 // Run one sweep over `targets` (all within one tile).  With grads_dev, the
@@ -396,8 +414,9 @@ static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
   const int n = psi->n;
   const int m = (int)tile_bits.size();
   const bool c64 = psi->dtype == MQ_C64;
-  const int lr = std::min(m, c64 ? 4 : 3);
-  const int maxph = (12 + (c64 ? 4 : 3) - 1) / (c64 ? 4 : 3);
+  const int lrt = adj_lr(psi->dtype);
+  const int lr = std::min(m, lrt);
+  const int maxph = std::min(kAdjMaxPhases, (12 + lrt - 1) / lrt);
   if ((int)targets.size() > maxph * lr) return fail(MQ_EINVAL, "too many targets for one adjoint sweep");
   AdjParams P;
   std::memset(&P, 0, sizeof(P));
@@ -408,7 +427,7 @@ static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
   for (int k = 0; k < m; ++k) P.tile_bit[k] = (uint8_t)tile_bits[k];
   {
     const int cb = c64 ? 1 : 0;
-    const int lt = std::min(7, m - lr);
+    const int lt = std::min(lrt == 3 ? 8 : 7, m - lr);
     const int first = cb + lt;
     bool contig = true;
     for (int b = first + 1; b < m; ++b)
@@ -470,7 +489,7 @@ static int run_adj_layer(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
   const int n = psi->n;
   const int tmax = std::min(kAdjTileMax, n);
   const int pas = 4;
-  const int lrt = psi->dtype == MQ_C64 ? 4 : 3;
+  const int lrt = adj_lr(psi->dtype);
   std::vector<std::pair<int, int>> groups;
   if (n <= tmax) {
     groups.push_back({0, n});
@@ -487,7 +506,7 @@ static int run_adj_layer(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
       start += cnt;
     }
   }
-  const size_t per = (size_t)((12 + lrt - 1) / lrt) * (size_t)std::min(lrt, tmax);
+  const size_t per = (size_t)std::min(kAdjMaxPhases, (12 + lrt - 1) / lrt) * (size_t)std::min(lrt, tmax);
   for (auto [start, cnt] : groups) {
     std::vector<AdjTarget> tg;
     std::vector<int> idx;

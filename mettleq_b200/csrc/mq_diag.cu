@@ -329,6 +329,76 @@ int plan_diag_windows(mq_state* h, int n_terms, const int32_t* kinds, const int3
   return MQ_OK;
 }
 
+// The diagonal split for a register phase whose register bits are rbits[4]
+// (ascending): phase(x) = W(x) * T[c(x)][r(x)] with r(x) the four register
+// bits, c(x) the values of the (at most 3) other bits that share a term with
+// a register bit, T the product of those terms, and W the remaining terms as
+// contiguous windows that do not read the register bits (so W can be taken
+// at the register group's base index).  out.n = -1 when this does not fit.
+int plan_diag_register(mq_state* h, int n_terms, const int32_t* kinds, const int32_t* wires, const double* params,
+                       const int* rbits, int max_entries, DiagRegister& out) {
+  std::vector<Term> terms;
+  std::complex<double> scalar;
+  int rc = build_terms(h->n, n_terms, kinds, wires, params, terms, scalar);
+  if (rc) return rc;
+  out = DiagRegister();
+  out.win.n = -1;
+  auto is_reg = [&](int b) { return b == rbits[0] || b == rbits[1] || b == rbits[2] || b == rbits[3]; };
+  std::vector<Term> group, reg;
+  std::vector<int> cross;
+  for (const Term& t : terms) {
+    bool touches = false;
+    for (int b : t.bits) touches = touches || is_reg(b);
+    if (!touches) { group.push_back(t); continue; }
+    reg.push_back(t);
+    for (int b : t.bits)
+      if (!is_reg(b) && std::find(cross.begin(), cross.end(), b) == cross.end()) cross.push_back(b);
+  }
+  if (cross.size() > 3) return MQ_OK;
+  std::sort(cross.begin(), cross.end());
+  // T[c][r]: value bit k of r = global bit rbits[k], bit j of c = cross[j]
+  std::vector<int> pos = {rbits[0], rbits[1], rbits[2], rbits[3]};
+  for (int b : cross) pos.push_back(b);
+  const uint32_t nt = 1u << pos.size();
+  std::vector<std::complex<double>> T(nt, scalar);
+  for (uint32_t x = 0; x < nt; ++x)
+    for (const Term& t : reg) T[x] *= term_value(t, pos, x);
+  // W: contiguous windows over the group terms
+  std::vector<PlannedLut> luts;
+  bool ok = false;
+  for (int W = 10; W >= 1 && !ok; --W) {
+    luts = plan_luts(group, W);
+    size_t entries = nt;
+    bool contig = true;
+    for (auto& L : luts) {
+      entries += L.vals.size();
+      contig = contig && L.contig && !L.pos.empty();
+    }
+    ok = contig && (int)luts.size() <= kMaxLuts && (int)entries <= max_entries;
+  }
+  if (!ok) return MQ_OK;
+  out.nc = (int)cross.size();
+  for (int j = 0; j < out.nc; ++j) out.cbit[j] = cross[j];
+  out.win.n = (int)luts.size();
+  uint32_t off = 0;
+  for (int l = 0; l < out.win.n; ++l) {
+    out.win.shift[l] = luts[l].pos[0];
+    out.win.nbits[l] = (int)luts[l].pos.size();
+    out.win.off[l] = (int)off;
+    for (auto v : luts[l].vals) {
+      out.win.vals.push_back(v.real());
+      out.win.vals.push_back(v.imag());
+    }
+    off += (uint32_t)luts[l].vals.size();
+  }
+  out.t_off = (int)off;
+  for (auto v : T) {
+    out.win.vals.push_back(v.real());
+    out.win.vals.push_back(v.imag());
+  }
+  return MQ_OK;
+}
+
 int launch_diag_terms(mq_state* h, int n_terms, const int32_t* kinds, const int32_t* wires, const double* params) {
   std::vector<Term> terms;
   std::complex<double> scalar;

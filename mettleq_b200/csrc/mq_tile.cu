@@ -48,7 +48,7 @@ constexpr int kMaxTileBits = 13;
 struct TileOp {
   uint8_t kind, phase, rk, lad_shift, width, pad[3];
   uint32_t cmask;  // OP_CU2: global index bits that must all be set
-  uint32_t pad2;
+  int32_t qubit;   // OP_U2 with device-resident matrices: row of mats_dev
   double u[8];     // 2x2 matrix (re, im interleaved)
 };
 
@@ -77,6 +77,10 @@ struct TileParams {
   uint32_t pad2;
   double scale;
   uint8_t ph_op[kMaxPhases + 2];     // QFT: ops of phase p are [ph_op[p], ph_op[p+1])
+  // U(2) matrices read from device memory at launch (mats_dev[8 q ..]):
+  // slot k of phase p takes row mat_q[p][k] - 1 (0 = the matrix in ph)
+  int16_t mat_q[kMaxPhases][5];
+  const double* mats_dev;
   PhaseDesc ph[kMaxPhases];
   TileOp ops[kMaxOps];
 };
@@ -92,6 +96,11 @@ constexpr int kEpiWin = 8;
 constexpr int kEpiLutBytes = 16384;
 struct EpiDesc {
   uint8_t diag, perm, n_win, n_var;
+  // dreg: the diagonal is applied in the last register phase instead:
+  // windows [0, n_win) at the group base times T[c][r] at lut[toff + 16c + r]
+  // (c = index bits cbit[0..nc))
+  uint8_t dreg, nc, cbit[3], pad0;
+  uint16_t toff, pad1;
   uint8_t shift[kEpiWin];
   uint8_t nbits[kEpiWin];
   uint16_t off[kEpiWin];
@@ -342,6 +351,20 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
     uint32_t* dstw = reinterpret_cast<uint32_t*>(phs);
     for (uint32_t w = tid; w < words; w += NT) dstw[w] = srcw[w];
   }
+  if constexpr (!QFT) {
+    if (P.mats_dev) {
+      __syncthreads();
+      for (int j = tid; j < P.n_phases * 40; j += NT) {
+        const int p = j / 40, k = (j / 8) % 5, e = j % 8;
+        const int q = P.mat_q[p][k] - 1;
+        if (q >= 0) {
+          const double v = P.mats_dev[(size_t)q * 8 + e];
+          phs[p].ud[k][e] = v;
+          phs[p].uf[k][e] = (float)v;
+        }
+      }
+    }
+  }
   if constexpr (EPI) {
     for (int w = tid; w < 32; w += NT) ecols[w] = P.epi.cols[w];
     const uint32_t words = P.epi.n_entries * (uint32_t)(sizeof(T) / 4);
@@ -461,6 +484,23 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
           if (D.any_ctl) apply_u2_phase<R, LR, true>(a, D, gq, greg);
           else apply_u2_phase<R, LR, false>(a, D, gq, greg);
         }
+        if constexpr (EPI && LR == 4) {
+          if (P.epi.dreg && ph == P.n_phases - 1) {
+            T f = mk<R>(1, 0);
+#pragma unroll
+            for (int w = 0; w < kEpiWin; ++w) {
+              if (w >= P.epi.n_win) break;
+              f = cmul(f, elut[P.epi.off[w] + ((gq >> P.epi.shift[w]) & ((1u << P.epi.nbits[w]) - 1u))]);
+            }
+            uint32_t cc = 0;
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+              if (j < P.epi.nc) cc |= ((gq >> P.epi.cbit[j]) & 1u) << j;
+            const T* tr = elut + P.epi.toff + (cc << 4);
+#pragma unroll
+            for (int r = 0; r < NR; ++r) a[r] = cmul(a[r], cmul(f, tr[r]));
+          }
+        }
         if (pair) {
 #pragma unroll
           for (int r = 0; r < NR; r += 2)
@@ -502,6 +542,7 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
 
 // ---------------------------------------------------------------- host side
 struct Sweep {
+  const double* mats_dev = nullptr;        // U(2) matrices in device memory (rows by qubit)
   std::vector<int> tile_bits;              // ascending global bits
   std::vector<std::vector<int>> phases;    // register bits (tile-local) per phase
   std::vector<TileOp> ops;
@@ -619,8 +660,9 @@ static int dispatch_tile(mq_state* h, const PT& P, size_t smem, bool oop) {
 
 // Fused-layer epilogue of a low sweep (see EpiDesc).
 struct EpiPlan {
-  bool diag = false, perm = false;
+  bool diag = false, perm = false, dreg = false;
   DiagWindows win;
+  DiagRegister reg;
   uint32_t cols[32] = {};
   uint32_t c = 0;
 };
@@ -632,6 +674,24 @@ static void fill_epi(EpiDesc& D, const EpiPlan& e, int m, int n) {
   if (e.perm) {
     for (int j = 0; j < n; ++j) D.cols[j] = e.cols[j];
     D.c = e.c;
+  }
+  if (e.dreg) {
+    const DiagRegister& G = e.reg;
+    D.dreg = 1;
+    D.n_win = (uint8_t)G.win.n;
+    D.nc = (uint8_t)G.nc;
+    for (int j = 0; j < G.nc; ++j) D.cbit[j] = (uint8_t)G.cbit[j];
+    for (int w = 0; w < G.win.n; ++w) {
+      D.shift[w] = (uint8_t)G.win.shift[w];
+      D.nbits[w] = (uint8_t)G.win.nbits[w];
+      D.off[w] = (uint16_t)G.win.off[w];
+    }
+    D.toff = (uint16_t)G.t_off;
+    R* vals = reinterpret_cast<R*>(D.lut);
+    const size_t cnt = G.win.vals.size() / 2;
+    for (size_t j = 0; j < 2 * cnt; ++j) vals[j] = (R)G.win.vals[j];
+    D.n_entries = (uint32_t)cnt;
+    return;
   }
   if (!e.diag) return;
   // windows overlapping the tile bits [0, m) first
@@ -728,6 +788,7 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
       const int k = op_rk[o];
       if (D.active & (1u << k)) return fail(MQ_EINVAL, "two gates on one register slot");
       D.active |= (uint8_t)(1u << k);
+      if (sw.mats_dev && sw.ops[o].kind == OP_U2) P.mat_q[op_phase[o]][k] = (int16_t)(sw.ops[o].qubit + 1);
       D.cmask[k] = sw.ops[o].kind == OP_CU2 ? sw.ops[o].cmask : 0u;
       if (D.cmask[k]) D.any_ctl = 1;
       for (int j = 0; j < 8; ++j) {
@@ -736,6 +797,7 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
       }
     }
   }
+  if (!qft) P.mats_dev = sw.mats_dev;
   P.need_tw = (qft && sw.need_tw && h->dtype == MQ_C64) ? 1 : 0;
   P.has_scale = sw.has_scale ? 1 : 0;
   P.scale = sw.has_scale ? sw.scale : 1.0;
@@ -798,7 +860,7 @@ static std::vector<std::pair<int, int>> split_bits(int n, int tmax, int pas) {
 // The U(2) sweep of index bits [start, start+cnt): targets are the active
 // qubits among them.  Returns false when none is active.
 static bool build_u2_sweep(mq_state* h, const double* mats, const uint8_t* active, int start, int cnt, Sweep& sw,
-                           std::vector<int>& op_phase, std::vector<int>& op_rk) {
+                           std::vector<int>& op_phase, std::vector<int>& op_rk, const double* mats_dev = nullptr) {
   const int n = h->n;
   std::vector<int> gbits, qubits;
   for (int b = start + cnt - 1; b >= start; --b) {
@@ -818,9 +880,12 @@ static bool build_u2_sweep(mq_state* h, const double* mats, const uint8_t* activ
     TileOp op;
     std::memset(&op, 0, sizeof(op));
     op.kind = OP_U2;
-    for (int j = 0; j < 8; ++j) op.u[j] = mats[(size_t)qubits[i] * 8 + j];
+    op.qubit = qubits[i];
+    if (mats)
+      for (int j = 0; j < 8; ++j) op.u[j] = mats[(size_t)qubits[i] * 8 + j];
     sw.ops.push_back(op);
   }
+  sw.mats_dev = mats ? nullptr : mats_dev;
   return true;
 }
 
@@ -846,7 +911,9 @@ int launch_u2_layer(mq_state* h, const double* mats, const uint8_t* active) {
 // contiguous windows, or a permutation that mixes the low bits with high
 // ones, runs as its own pass after the sweep.
 int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_terms, const int32_t* kinds,
-                 const int32_t* wires, const double* params, const uint32_t* cols, uint32_t c) {
+                 const int32_t* wires, const double* params, const uint32_t* cols, uint32_t c,
+                 const double* mats_dev) {
+  const bool u2 = mats || mats_dev;
   const int n = h->n;
   if (cols) {
     uint32_t inv[32];
@@ -856,16 +923,28 @@ int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_t
   // low sweep plan first, so that argument errors surface before any launch
   Sweep low;
   std::vector<int> low_phase, low_rk;
-  const bool low_u2 = mats && build_u2_sweep(h, mats, active, groups[0].first, groups[0].second, low, low_phase, low_rk);
+  const bool low_u2 = u2 && build_u2_sweep(h, mats, active, groups[0].first, groups[0].second, low, low_phase, low_rk,
+                                           mats_dev);
   if (!low_u2) low.tile_bits = tile_for(n, {0}, passengers(), tile_max(h->dtype));
   const int m = (int)low.tile_bits.size();
   EpiPlan e;
   if (n_terms > 0) {
-    int rc = plan_diag_windows(h, n_terms, kinds, wires, params, kEpiLutBytes / (int)h->amp_bytes(), e.win);
-    if (rc) return rc;
-    e.diag = e.win.n > 0;
+    const int max_entries = kEpiLutBytes / (int)h->amp_bytes();
+    // preferred: the diagonal in the last register phase of the low sweep
+    if (low_u2 && !low.phases.empty() && low.phases.back().size() == 4 && m >= 4) {
+      const auto& regs = low.phases.back();
+      const int rb[4] = {regs[0], regs[1], regs[2], regs[3]};
+      int rc = plan_diag_register(h, n_terms, kinds, wires, params, rb, max_entries, e.reg);
+      if (rc) return rc;
+      e.dreg = e.reg.win.n >= 0;
+    }
+    if (!e.dreg) {
+      int rc = plan_diag_windows(h, n_terms, kinds, wires, params, max_entries, e.win);
+      if (rc) return rc;
+      e.diag = e.win.n > 0;
+    }
   }
-  const bool diag_separate = n_terms > 0 && !e.diag;
+  const bool diag_separate = n_terms > 0 && !e.diag && !e.dreg;
   if (cols && !diag_separate) {
     e.perm = true;
     for (int j = 0; j < m; ++j)
@@ -877,17 +956,17 @@ int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_t
       if (rc) return rc;
     }
   }
-  if (mats) {
+  if (u2) {
     for (size_t g = 1; g < groups.size(); ++g) {
       Sweep sw;
       std::vector<int> op_phase, op_rk;
-      if (!build_u2_sweep(h, mats, active, groups[g].first, groups[g].second, sw, op_phase, op_rk)) continue;
+      if (!build_u2_sweep(h, mats, active, groups[g].first, groups[g].second, sw, op_phase, op_rk, mats_dev)) continue;
       int rc = run_sweep(h, sw, op_phase, op_rk);
       if (rc) return rc;
     }
   }
-  if (low_u2 || e.diag || e.perm) {
-    int rc = run_sweep(h, low, low_phase, low_rk, (e.diag || e.perm) ? &e : nullptr);
+  if (low_u2 || e.diag || e.perm || e.dreg) {
+    int rc = run_sweep(h, low, low_phase, low_rk, (e.diag || e.perm || e.dreg) ? &e : nullptr);
     if (rc) return rc;
   }
   if (diag_separate) {
