@@ -171,6 +171,29 @@ int mq_adjoint_layer(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubit
 int mq_adjoint_layer_async(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits,
                            const double* mats, double* out_dev);
 
+/* ---- batched circuits (integrations/qiskit.py:505-514 runs them one by one) */
+/* A batch of layered circuits: circuit c has n_qubits[c] qubits (1..30) and
+ * depth[c] layers, each a 2x2 on every qubit followed (ladder[c] != 0, or
+ * ladder == NULL) by CNOT(0,1), ..., CNOT(n-2,n-1).  Circuits of <= 13 qubits
+ * run whole in shared memory (small_threads: 128, 256 or 512 threads per
+ * block); larger ones run tile sweeps on `lanes` parallel streams.  The
+ * first run captures everything as one CUDA graph; later runs with the same
+ * output pointers replay it. */
+typedef struct mq_batch mq_batch;
+int mq_batch_create(int device, void* stream, int n_circuits, const int32_t* n_qubits,
+                    const int32_t* depth, const uint8_t* ladder, int lanes, int small_threads,
+                    mq_batch** out);
+/* mats_count = total doubles of mq_batch_run's mats; probs_count = sum of 2^n. */
+int mq_batch_info(const mq_batch* b, uint64_t* mats_count, uint64_t* probs_count,
+                  int* n_small, int* n_large);
+/* mats (host): for every circuit in order, depth x n x 8 doubles (layer,
+ * qubit, [u00,u01,u10,u11] re/im).  probs_dev (device, float32): every
+ * circuit's full probability vector in order (first qubit = MSB); z0_dev
+ * (device, float64): <Z_0> per circuit.  Asynchronous on the batch stream. */
+int mq_batch_run(mq_batch* b, const double* mats, float* probs_dev, double* z0_dev);
+int mq_batch_sync(mq_batch* b);
+int mq_batch_destroy(mq_batch* b);
+
 /* mq_expval_pauli without any device allocation.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc or cudaFree
  * in the middle of their work -- a serving loop that admits requests by

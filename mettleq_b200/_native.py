@@ -56,6 +56,11 @@ SIGNATURES = {
     "mq_sample": (_I, [_P, _P, _I, _U64, _U64, _I64, _P]),
     "mq_expval_pauli": (_I, [_P, _I, _P, _P, _P, _P]),
     "mq_expval_pauli_static": (_I, [_P, _I, _P, _P, _P, _P]),
+    "mq_batch_create": (_I, [_I, _P, _I, _P, _P, _P, _I, _I, C.POINTER(_P)]),
+    "mq_batch_info": (_I, [_P, C.POINTER(_U64), C.POINTER(_U64), C.POINTER(_I), C.POINTER(_I)]),
+    "mq_batch_run": (_I, [_P, _P, _P, _P]),
+    "mq_batch_sync": (_I, [_P]),
+    "mq_batch_destroy": (_I, [_P]),
     "mq_apply_pauli_sum": (_I, [_P, _P, _I, _P, _P, _P, _P]),
     "mq_adjoint_layer": (_I, [_P, _P, _I, _P, _P, _P]),
     "mq_adjoint_layer_async": (_I, [_P, _P, _I, _P, _P, _P]),
