@@ -44,6 +44,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["scale", "batch", "adjoint", "serve"], default="scale",
+                    help="scale (the headline line), batch (4096 mixed circuits in one graph), adjoint "
+                         "(24-qubit gradient of 384 parameters), serve (Poisson request stream)")
+    ap.add_argument("--count", type=int, default=None, help="circuits (batch) or requests (serve)")
     ap.add_argument("--qubits", type=int, default=30)
     ap.add_argument("--layers", type=int, default=40)
     ap.add_argument("--seed", type=int, default=0)
@@ -170,6 +174,7 @@ def run_ours(args, rank, world, local_rank, dist):
     from mettleq_b200 import workloads as W
     from mettleq_b200.engine import StateVector
     from mettleq_b200.device import Device
+    from mettleq_b200.replicas import max_over_ranks
 
     torch.cuda.set_device(local_rank)
     # a dedicated (non-default) stream: libmq launches on it and the CUDA
@@ -232,11 +237,7 @@ def run_ours(args, rank, world, local_rank, dist):
     clk = clocks.stop()
     if dist:
         dist.barrier()
-    elapsed = start.elapsed_time(end) / 1000.0
-    if dist:
-        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(start.elapsed_time(end) / 1000.0, dist, device="cuda")
     per_kind = {k: sum(a.elapsed_time(b) for a, b in v) / 1000.0 for k, v in spans.items()}
     counts = {k: len(v) for k, v in spans.items()}
     launches = c1[0] - c0[0]
@@ -325,11 +326,7 @@ def run_ours(args, rank, world, local_rank, dist):
             e2e_step(i + 1)
         e1.record(stream)
         torch.cuda.synchronize()
-        te = e0.elapsed_time(e1) / 1000.0
-        if dist:
-            t = torch.tensor([te], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
+        te = max_over_ranks(e0.elapsed_time(e1) / 1000.0, dist, device="cuda")
         h2d = (dev.sim.param_bytes - p0) / k
         out["e2e"] = {"value": world * k * logical * layer_bytes / te / 1e9, "unit": "GB/s",
                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(args.shots * 8 + 16),
@@ -345,6 +342,180 @@ def run_ours(args, rank, world, local_rank, dist):
         out["cpu_baseline"] = {"value": logical * layer_bytes / t_cpu / 1e9, "unit": "GB/s", "cores": 1,
                                "kind": "port", "sample": sample, "extrapolated_circuit_s": t_cpu}
     return out
+
+
+# ---------------------------------------------------------------- other workloads
+def _timed_clocks(fn):
+    clocks = ClockSampler(0)
+    clocks.start()
+    try:
+        r = fn()
+    finally:
+        clk = clocks.stop()
+    return r, clk
+
+
+def run_batch(args):
+    """4096 hardware-efficient-ansatz circuits (n ~ U{10..24}, depth ~ U{4..16},
+    RY/RZ angles U[-pi, pi], CNOT ladder), complex64, outputs <Z_0> and every
+    probability vector on the device, in one CUDA-graph launch; beside it the
+    plain path (one circuit at a time through Device.execute + probabilities)
+    on a sample of the same circuits."""
+    import torch
+    from mettleq_b200.batch import CircuitBatch, autotune, hea_batch, hea_mats, hea_ops
+    from mettleq_b200.device import Device
+    count = args.count or 4096
+    ns, ds, ps = hea_batch(count, seed=args.seed)
+    mats = [hea_mats(p) for p in ps]
+    sub = list(range(0, count, max(1, count // 512)))
+    b0 = CircuitBatch([ns[i] for i in sub], [ds[i] for i in sub])
+    packed_sub = b0.pack([mats[i] for i in sub])
+    b0.close()
+    t0 = time.perf_counter()
+    tune = autotune([ns[i] for i in sub], [ds[i] for i in sub], packed_sub)
+    tune_s = time.perf_counter() - t0
+    b = CircuitBatch(ns, ds, lanes=tune["lanes"], small_threads=tune["small_threads"])
+    packed = b.pack(mats)
+    t0 = time.perf_counter()
+    b.run(packed=packed)
+    b.synchronize()
+    capture_s = time.perf_counter() - t0
+    for _ in range(max(0, args.warmup - 1)):
+        b.run(packed=packed)
+    b.synchronize()
+    stream = torch.cuda.Stream()
+
+    def timed():
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            b.run(packed=packed)   # host copy of the matrices + graph launch
+            b.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return ts
+
+    ts, clk = _timed_clocks(timed)
+    t_run = statistics.median(ts)
+    z0 = b.z0()
+    # plain path on a sample
+    sample = list(range(0, count, max(1, count // 256)))
+    devs = {}
+    err = 0.0
+    t0 = time.perf_counter()
+    for i in sample:
+        n = ns[i]
+        if n not in devs:
+            devs[n] = Device(n)
+        d = devs[n]
+        d.reset()
+        d.execute(hea_ops(ps[i]))
+        pr = d.sim.probabilities(dtype=np.float32)
+        z = float(pr[: len(pr) // 2].sum() - pr[len(pr) // 2:].sum())
+        err = max(err, abs(z - z0[i]))
+    t_plain = time.perf_counter() - t0
+    for d in devs.values():
+        d.close()
+    b.close()
+    plain_cps = len(sample) / t_plain
+    value = count / t_run
+    return {
+        "metric": "batched circuits/s", "value": value, "unit": "circuits/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_run * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded hardware-efficient ansatz)",
+        "config": {"workload": f"batch: {count} circuits, n ~ U{{10..24}}, depth ~ U{{4..16}}, RY+RZ on every qubit "
+                               "then CNOT ladder; outputs <Z_0> and full probabilities (float32, on device)",
+                   "sum_state_GB": sum((1 << n) * 8 for n in ns) / 1e9, "small_circuits": b.n_small,
+                   "large_circuits": b.n_large},
+        "step": "host copy of all matrices + one CUDA-graph launch (graph captured once, untimed)",
+        "capture_first_run_s": capture_s, "autotune": dict(tune, seconds=tune_s),
+        "plain": {"circuits_per_s": plain_cps, "sample": len(sample),
+                  "path": "Device.execute(op dicts) + probabilities to host, one circuit at a time"},
+        "speedup_vs_plain": value / plain_cps, "z0_max_diff_vs_plain": err, "clocks": clk,
+    }
+
+
+def run_adjoint(args):
+    """Adjoint gradient of E = <H>, H = sum Z_i Z_{i+1} + 0.5 sum X_i, for 8
+    layers of RY+RZ on 24 qubits + CNOT ladder (384 parameters), complex64,
+    against one forward pass (circuit + energy)."""
+    import torch
+    from mettleq_b200.adjoint import AdjointEngine, LayeredAnsatz, PauliSum
+    n = 24 if args.qubits == 30 else args.qubits
+    A = LayeredAnsatz(n, 8)
+    H = PauliSum.ising_chain(n)
+    p = np.random.default_rng(args.seed).uniform(-math.pi, math.pi, A.shape)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    eng = AdjointEngine(A, H, dtype="complex64", stream=stream.cuda_stream)
+
+    def t(fn):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts)
+
+    def measure():
+        return t(lambda: eng.energy(p)), t(lambda: eng.energy_and_grad(p))
+
+    (tf, tg), clk = _timed_clocks(measure)
+    e, g = eng.energy_and_grad(p)
+    # spot check against the parameter-shift rule on the same engine
+    flat = p.reshape(-1)
+    idx = [0, 100, 200, 383]
+    ps_err = 0.0
+    for i in idx:
+        q = flat.copy()
+        q[i] += math.pi / 2
+        ep = eng.energy(q.reshape(A.shape))
+        q[i] -= math.pi
+        em = eng.energy(q.reshape(A.shape))
+        ps_err = max(ps_err, abs(0.5 * (ep - em) - g.reshape(-1)[i]))
+    eng.close()
+    return {
+        "metric": "adjoint gradient time / forward time", "value": (tg - tf) / tf, "unit": "x",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": tg * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+        "config": {"workload": f"adjoint: {n} qubits, 8 layers RY+RZ + CNOT ladder ({p.size} parameters), "
+                               "H = sum Z_i Z_i+1 + 0.5 sum X_i"},
+        "forward_ms": tf * 1e3, "forward_plus_gradient_ms": tg * 1e3, "gradient_only_ms": (tg - tf) * 1e3,
+        "total_over_forward": tg / tf, "energy": e, "param_shift_max_diff": ps_err, "clocks": clk,
+    }
+
+
+def run_serve(args):
+    """Poisson stream at 200 requests/s, n log-uniform in [12, 30], depth
+    U{10..100} config-0 layers (QFT and GF(2) layer each with p = 0.1), 1000
+    shots, complex64, 150 GB admission budget; beside it the plain path (one
+    request at a time through Device.execute) on the first requests."""
+    from mettleq_b200.serving import Server, poisson_requests, serve_plain
+    count = args.count or 200
+    reqs = poisson_requests(count, rate=200.0, seed=args.seed)
+    srv = Server(budget_bytes=150 * 10 ** 9)
+    srv.serve(poisson_requests(8, seed=99, n_range=(12, 16), depth_range=(2, 3)), realtime=False)
+    stats, clk = _timed_clocks(lambda: srv.serve(reqs, realtime=True))
+    peak, active = srv.peak_used, srv.peak_active
+    srv.close()
+    plain_n = max(1, count // 5)
+    plain = serve_plain(poisson_requests(count, rate=200.0, seed=args.seed)[:plain_n], realtime=True)
+    return {
+        "metric": "serve p50 latency", "value": stats["p50_s"], "unit": "s", "n_gpus": 1, "steps": 1,
+        "warmup": 1, "ms_per_step": stats["makespan_s"] * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded Poisson request stream)",
+        "config": {"workload": f"serve: {count} requests, Poisson 200 req/s, n log-uniform 12..30, depth U{{10..100}}, "
+                               "QFT/XOR p=0.1, 1000 shots, 150 GB budget"},
+        "p99_s": stats["p99_s"], "mean_s": stats["mean_s"], "circuits_per_s": stats["circuits_per_s"],
+        "peak_admitted_GB": peak / 1e9, "peak_active": active,
+        "plain": dict(plain, path="one request at a time: Device.execute(op dicts) + seeded shots"),
+        "throughput_vs_plain": stats["circuits_per_s"] / plain["circuits_per_s"], "clocks": clk,
+    }
 
 
 # ---------------------------------------------------------------- reference arm
@@ -382,6 +553,11 @@ def main():
         if rank != 0:
             return 0
         print(json.dumps(run_reference(args)), flush=True)
+        return 0
+    if args.workload != "scale":
+        if rank == 0:
+            fn = {"batch": run_batch, "adjoint": run_adjoint, "serve": run_serve}[args.workload]
+            print(json.dumps(fn(args)), flush=True)
         return 0
     dist = None
     if world > 1:

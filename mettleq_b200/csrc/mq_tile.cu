@@ -112,6 +112,13 @@ struct EpiDesc {
 struct FusedParams : TileParams {
   EpiDesc epi;
 };
+// QFT sweeps: per stage op, the phase factor of each register pattern r
+// (e^{i pi Lr(r) / 2^width}, see apply_qft).
+struct QftParams : TileParams {
+  alignas(16) float2 twf[kMaxOps][32];
+  alignas(16) double2 twd[kMaxOps][32];
+};
+static_assert(sizeof(QftParams) <= 32000, "kernel parameter block too large");
 static_assert(sizeof(FusedParams) <= 32000, "kernel parameter block too large");
 
 // e^{i pi L / 2^width}, 1 <= width <= 31, L < 2^width.
@@ -189,30 +196,36 @@ __device__ __forceinline__ void apply_u2_phase(V2<R> (&a)[1 << LR], const PhaseD
 }
 
 // One QFT stage on register bit K (forward: butterfly then phase; inverse:
-// conjugate phase then butterfly).
+// conjugate phase then butterfly).  The phase of the bit-1 half is
+// e^{i pi L / 2^w} with L = Lg + Lr: Lg from the group's index bits (one
+// Twiddle per group), Lr from the register bits, whose factor treg[r] the
+// host tabulates per stage, so a pair costs one complex product for its
+// phase.
 template <typename R, int LR, int K>
-__device__ __forceinline__ void apply_qft(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const uint32_t* greg,
+__device__ __forceinline__ void apply_qft(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const V2<R>* treg,
                                           const float2* tw) {
   using T = V2<R>;
   constexpr int NR = 1 << LR;
   const int width = op.width;
-  const int shift = op.lad_shift;
-  const uint32_t mask = width ? ((width >= 32) ? 0xffffffffu : ((1u << width) - 1u)) : 0u;
   const bool fwd = op.kind == OP_QFT_FWD;
+  T tg = mk<R>(1, 0);
+  if (width) {
+    const uint32_t mask = (width >= 32) ? 0xffffffffu : ((1u << width) - 1u);
+    const uint32_t Lg = (gq >> op.lad_shift) & mask;
+    if (Lg) tg = Twiddle<R>::get(tw, Lg, width);
+  }
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
     if (r & (1 << K)) continue;
     const int r1 = r | (1 << K);
     T x0 = a[r], x1 = a[r1];
-    uint32_t L = 0;
-    if (width) L = ((gq | osel<LR>(r1, greg)) >> shift) & mask;
     if (fwd) {
       T d = csub(x0, x1);
       a[r] = cadd(x0, x1);
-      if (L) d = cmul(d, Twiddle<R>::get(tw, L, width));
+      if (width) d = cmul(d, cmul(tg, treg[r1]));
       a[r1] = d;
     } else {
-      if (L) x1 = cmulc(x1, Twiddle<R>::get(tw, L, width));
+      if (width) x1 = cmulc(x1, cmul(tg, treg[r1]));
       a[r] = cadd(x0, x1);
       a[r1] = csub(x0, x1);
     }
@@ -220,14 +233,14 @@ __device__ __forceinline__ void apply_qft(V2<R> (&a)[1 << LR], const TileOp& op,
 }
 
 template <typename R, int LR>
-__device__ __forceinline__ void apply_qft_op(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const uint32_t* greg,
+__device__ __forceinline__ void apply_qft_op(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const V2<R>* treg,
                                              const float2* tw) {
   switch (op.rk) {
-    case 0: apply_qft<R, LR, 0>(a, op, gq, greg, tw); break;
-    case 1: if constexpr (LR > 1) apply_qft<R, LR, 1>(a, op, gq, greg, tw); break;
-    case 2: if constexpr (LR > 2) apply_qft<R, LR, 2>(a, op, gq, greg, tw); break;
-    case 3: if constexpr (LR > 3) apply_qft<R, LR, 3>(a, op, gq, greg, tw); break;
-    case 4: if constexpr (LR > 4) apply_qft<R, LR, 4>(a, op, gq, greg, tw); break;
+    case 0: apply_qft<R, LR, 0>(a, op, gq, treg, tw); break;
+    case 1: if constexpr (LR > 1) apply_qft<R, LR, 1>(a, op, gq, treg, tw); break;
+    case 2: if constexpr (LR > 2) apply_qft<R, LR, 2>(a, op, gq, treg, tw); break;
+    case 3: if constexpr (LR > 3) apply_qft<R, LR, 3>(a, op, gq, treg, tw); break;
+    case 4: if constexpr (LR > 4) apply_qft<R, LR, 4>(a, op, gq, treg, tw); break;
     default: break;
   }
 }
@@ -479,7 +492,12 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
           for (int r = 0; r < NR; ++r) a[r] = cur[sq ^ osel<LR>(r, sreg)];
         }
         if constexpr (QFT) {
-          for (int o = P.ph_op[ph]; o < P.ph_op[ph + 1]; ++o) apply_qft_op<R, LR>(a, P.ops[o], gq, greg, tw);
+          for (int o = P.ph_op[ph]; o < P.ph_op[ph + 1]; ++o) {
+            const V2<R>* treg;
+            if constexpr (sizeof(R) == 4) treg = P.twf[o];
+            else treg = P.twd[o];
+            apply_qft_op<R, LR>(a, P.ops[o], gq, treg, tw);
+          }
         } else {
           if (D.any_ctl) apply_u2_phase<R, LR, true>(a, D, gq, greg);
           else apply_u2_phase<R, LR, false>(a, D, gq, greg);
@@ -811,9 +829,29 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
     if (h->dtype == MQ_C64) return dispatch_tile<float, 2>(h, F, smem, epi->perm);
     return dispatch_tile<double, 2>(h, F, smem, epi->perm);
   }
-  if (h->dtype == MQ_C64)
-    return qft ? dispatch_tile<float, 1>(h, P, smem, false) : dispatch_tile<float, 0>(h, P, smem, false);
-  return qft ? dispatch_tile<double, 1>(h, P, smem, false) : dispatch_tile<double, 0>(h, P, smem, false);
+  if (qft) {
+    QftParams Q;
+    std::memset(&Q, 0, sizeof(Q));
+    static_cast<TileParams&>(Q) = P;
+    for (int w = 0; w < P.n_ops; ++w) {
+      const TileOp& op = P.ops[w];
+      const PhaseDesc& D = P.ph[op.phase];
+      const uint32_t mask = op.width >= 32 ? 0xffffffffu : ((1u << op.width) - 1u);
+      for (int r = 0; r < (1 << lr); ++r) {
+        uint64_t Lr = 0;
+        for (int k = 0; k < lr; ++k)
+          if ((r >> k) & 1) Lr += (D.g_reg[k] >> op.lad_shift) & mask;
+        const double ang = op.width ? M_PI * std::ldexp((double)Lr, -op.width) : 0.0;
+        const double c = std::cos(ang), sn = std::sin(ang);
+        Q.twf[w][r] = make_float2((float)c, (float)sn);
+        Q.twd[w][r] = make_double2(c, sn);
+      }
+    }
+    if (h->dtype == MQ_C64) return dispatch_tile<float, 1>(h, Q, smem, false);
+    return dispatch_tile<double, 1>(h, Q, smem, false);
+  }
+  if (h->dtype == MQ_C64) return dispatch_tile<float, 0>(h, P, smem, false);
+  return dispatch_tile<double, 0>(h, P, smem, false);
 }
 
 static int tile_local(const std::vector<int>& bits, int gbit) {
