@@ -30,9 +30,12 @@
 #include <algorithm>
 #include <cstddef>
 #include <cmath>
+#include <complex>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "mq_internal.cuh"
@@ -63,6 +66,7 @@ struct __align__(16) PhaseDesc {
   uint32_t cmask[5];     // controls of the slot's gate (0 = none)
   uint8_t active;        // slots carrying a gate
   uint8_t any_ctl;       // some slot is controlled
+  uint8_t real;          // slots whose matrix is real (RY-type: 2 FMA per output component)
   alignas(16) float uf[5][8];   // rows read as two 16-byte vectors
   alignas(16) double ud[5][8];
 };
@@ -94,7 +98,18 @@ struct TileParams {
 // over a tile and multiplied once per tile.
 constexpr int kEpiWin = 8;
 constexpr int kEpiLutBytes = 16384;
+// A diagonal applied to a 4-bit register phase: windows [0, n_win) taken at
+// the group base, times T[c][r] at lut[toff + 16c + r] (c = index bits
+// cbit[0..nc)).
+struct RegDiag {
+  uint8_t on, nc, cbit[3], n_win, pad[2];
+  uint8_t shift[kEpiWin];
+  uint8_t nbits[kEpiWin];
+  uint16_t off[kEpiWin];
+  uint16_t toff, pad1;
+};
 struct EpiDesc {
+  RegDiag pre;  // applied in the first register phase, before its gates
   uint8_t diag, perm, n_win, n_var;
   // dreg: the diagonal is applied in the last register phase instead:
   // windows [0, n_win) at the group base times T[c][r] at lut[toff + 16c + r]
@@ -174,6 +189,20 @@ __device__ __forceinline__ void apply_u2(V2<R> (&a)[1 << LR], const PhaseDesc& D
     u10 = mk<R>(D.ud[K][4], D.ud[K][5]); u11 = mk<R>(D.ud[K][6], D.ud[K][7]);
   }
   const uint32_t cm = D.cmask[K];
+  if (!CTL && ((D.real >> K) & 1u)) {
+    // real matrix: each output component is two products
+    const R c00 = u00.x, c01 = u01.x, c10 = u10.x, c11 = u11.x;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      if (r & (1 << K)) continue;
+      const T x0 = a[r], x1 = a[r | (1 << K)];
+      a[r].x = fma(c00, x0.x, c01 * x1.x);
+      a[r].y = fma(c00, x0.y, c01 * x1.y);
+      a[r | (1 << K)].x = fma(c10, x0.x, c11 * x1.x);
+      a[r | (1 << K)].y = fma(c10, x0.y, c11 * x1.y);
+    }
+    return;
+  }
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
     if (r & (1 << K)) continue;
@@ -310,6 +339,24 @@ __device__ __forceinline__ void epilogue_store(const EpiDesc& D, const V2<R>* cu
   }
 }
 
+template <typename R>
+__device__ __forceinline__ void apply_regdiag(V2<R> (&a)[16], const V2<R>* lut, const RegDiag& D, uint32_t gq) {
+  using T = V2<R>;
+  T f = mk<R>(1, 0);
+#pragma unroll
+  for (int w = 0; w < kEpiWin; ++w) {
+    if (w >= D.n_win) break;
+    f = cmul(f, lut[D.off[w] + ((gq >> D.shift[w]) & ((1u << D.nbits[w]) - 1u))]);
+  }
+  uint32_t cc = 0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+    if (j < D.nc) cc |= ((gq >> D.cbit[j]) & 1u) << j;
+  const T* tr = lut + D.toff + (cc << 4);
+#pragma unroll
+  for (int r = 0; r < 16; ++r) a[r] = cmul(a[r], cmul(f, tr[r]));
+}
+
 template <int M>
 __device__ __forceinline__ uint32_t tile_base_of(uint32_t tile, const TileParams& P) {
   uint64_t x = tile;
@@ -336,7 +383,7 @@ __device__ __forceinline__ uint32_t tile_base_of(uint32_t tile, const TileParams
 // MODE 0: U(2) / controlled U(2) phases; MODE 1: QFT stages; MODE 2: U(2)
 // phases plus the fused-layer epilogue (PT = FusedParams, tile bits [0, M)).
 template <typename R, int M, int LR, int LT, int MODE, typename PT>
-__global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? 3 : (LT >= 7 ? (sizeof(R) == 4 && LR == 4 ? 6 : 3) : (LT >= 6 && sizeof(R) == 4 ? 8 : 1)))))
+__global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? (MODE == 2 ? 2 : 3) : (LT >= 7 ? (sizeof(R) == 4 && LR == 4 ? 6 : 3) : (LT >= 6 && sizeof(R) == 4 ? 8 : 1)))))
 k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   using T = V2<R>;
   constexpr bool QFT = MODE == 1;
@@ -427,8 +474,8 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   auto src_base = [&](uint32_t t, uint32_t& cl) -> uint32_t {
     cl = 0;
     if constexpr (EPI) {
+      if (!P.epi.perm) return tile_base_of<M>(t, P);
       const uint32_t bo = t << M;
-      if (!P.epi.perm) return bo;
       uint32_t b = P.epi.c;
       for (int j = M; j < (int)P.n; ++j)
         if ((bo >> j) & 1u) b ^= ecols[j];
@@ -491,6 +538,9 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
 #pragma unroll
           for (int r = 0; r < NR; ++r) a[r] = cur[sq ^ osel<LR>(r, sreg)];
         }
+        if constexpr (EPI && LR == 4) {
+          if (P.epi.pre.on && ph == 0) apply_regdiag<R>(a, elut, P.epi.pre, gq);
+        }
         if constexpr (QFT) {
           for (int o = P.ph_op[ph]; o < P.ph_op[ph + 1]; ++o) {
             const V2<R>* treg;
@@ -532,9 +582,11 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
       __syncthreads();
     }
     if constexpr (EPI) {
-      epilogue_store<R, M, LT, CPT>(P.epi, cur, ecols, elut, dst, tile << M, base, cl_in, tid);
-      __syncthreads();
-      continue;
+      if (P.epi.perm || P.epi.diag) {
+        epilogue_store<R, M, LT, CPT>(P.epi, cur, ecols, elut, dst, tile << M, base, cl_in, tid);
+        __syncthreads();
+        continue;
+      }
     }
     const uint32_t gb = base | g_t;
     const float4* c4 = reinterpret_cast<const float4*>(cur);
@@ -586,6 +638,11 @@ static int tile_max(int dtype) {
   return env_int("MQ_TILE_MAX", 12, 6, lim);
 }
 static int passengers() { return env_int("MQ_TILE_PASSENGERS", 4, 0, 5); }
+static bool euler_enabled(const mq_state* h) {
+  const char* v = std::getenv("MQ_EULER");
+  if (v && v[0] == '0') return false;
+  return h->n >= env_int("MQ_EULER_MIN_QUBITS", 16, 1, 32);
+}
 static int min_tile() { return env_int("MQ_TILE_MIN", 10, 1, 12); }
 
 // Register phases: targets (tile-local) chunked in the given order into
@@ -618,12 +675,26 @@ static void make_phases(int m, int lr, const std::vector<int>& order, Sweep& sw,
 template <typename R, int M, int LR, int LT, int MODE, typename PT>
 static int launch_tile_t(mq_state* h, const PT& P, size_t smem, bool out_of_place) {
   auto kern = k_tile<R, M, LR, LT, MODE, PT>;
+  // the opt-in shared-memory limit only grows; resident CTAs per SM depend on
+  // this launch's shared memory (rounded up to 1 KiB), looked up per size
+  static std::mutex mu;
   static int configured_smem = -1;
-  static int blocks_per_sm = 0;
-  if ((int)smem > configured_smem) {
-    MQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
-    configured_smem = (int)std::max<size_t>(smem, 48 * 1024);
-    MQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, 1 << LT, smem));
+  static std::map<size_t, int> occupancy;
+  int blocks_per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    const size_t key = (smem + 1023) & ~size_t(1023);
+    if ((int)key > configured_smem) {
+      MQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(key, 48 * 1024)));
+      configured_smem = (int)std::max<size_t>(key, 48 * 1024);
+    }
+    auto it = occupancy.find(key);
+    if (it == occupancy.end()) {
+      MQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, 1 << LT, key));
+      occupancy[key] = blocks_per_sm;
+    } else {
+      blocks_per_sm = it->second;
+    }
   }
   const uint32_t grid = (uint32_t)std::max<uint64_t>(
       1, std::min<uint64_t>(P.n_tiles, (uint64_t)h->num_sms * std::max(1, blocks_per_sm)));
@@ -678,12 +749,32 @@ static int dispatch_tile(mq_state* h, const PT& P, size_t smem, bool oop) {
 
 // Fused-layer epilogue of a low sweep (see EpiDesc).
 struct EpiPlan {
-  bool diag = false, perm = false, dreg = false;
+  bool diag = false, perm = false, dreg = false, pre = false;
   DiagWindows win;
-  DiagRegister reg;
+  DiagRegister reg;      // dreg: after the last register phase's gates
+  DiagRegister pre_reg;  // pre: before the first register phase's gates
   uint32_t cols[32] = {};
   uint32_t c = 0;
 };
+
+// Copies a register-phase diagonal's tables to vals[base..] and its
+// descriptor into RD (offsets relative to the whole table array).
+template <typename R>
+static uint32_t fill_regdiag(RegDiag& RD, const DiagRegister& G, R* vals, uint32_t base) {
+  RD.on = 1;
+  RD.n_win = (uint8_t)G.win.n;
+  RD.nc = (uint8_t)G.nc;
+  for (int j = 0; j < G.nc; ++j) RD.cbit[j] = (uint8_t)G.cbit[j];
+  for (int w = 0; w < G.win.n; ++w) {
+    RD.shift[w] = (uint8_t)G.win.shift[w];
+    RD.nbits[w] = (uint8_t)G.win.nbits[w];
+    RD.off[w] = (uint16_t)(base + G.win.off[w]);
+  }
+  RD.toff = (uint16_t)(base + G.t_off);
+  const size_t cnt = G.win.vals.size() / 2;
+  for (size_t j = 0; j < 2 * cnt; ++j) vals[2 * base + j] = (R)G.win.vals[j];
+  return base + (uint32_t)cnt;
+}
 
 template <typename R>
 static void fill_epi(EpiDesc& D, const EpiPlan& e, int m, int n) {
@@ -692,6 +783,13 @@ static void fill_epi(EpiDesc& D, const EpiPlan& e, int m, int n) {
   if (e.perm) {
     for (int j = 0; j < n; ++j) D.cols[j] = e.cols[j];
     D.c = e.c;
+  }
+  uint32_t used = 0;
+  if (e.pre) {
+    // after the post tables when both are present
+    const uint32_t base = e.dreg ? (uint32_t)(e.reg.win.vals.size() / 2) : 0u;
+    used = fill_regdiag<R>(D.pre, e.pre_reg, reinterpret_cast<R*>(D.lut), base);
+    D.n_entries = used;
   }
   if (e.dreg) {
     const DiagRegister& G = e.reg;
@@ -708,9 +806,10 @@ static void fill_epi(EpiDesc& D, const EpiPlan& e, int m, int n) {
     R* vals = reinterpret_cast<R*>(D.lut);
     const size_t cnt = G.win.vals.size() / 2;
     for (size_t j = 0; j < 2 * cnt; ++j) vals[j] = (R)G.win.vals[j];
-    D.n_entries = (uint32_t)cnt;
+    D.n_entries = std::max<uint32_t>(used, (uint32_t)cnt);
     return;
   }
+  if (e.pre) return;
   if (!e.diag) return;
   // windows overlapping the tile bits [0, m) first
   std::vector<int> order;
@@ -744,7 +843,7 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
   if (m < 1 || m > tile_max(h->dtype) || m > h->n) return fail(MQ_EINVAL, "bad tile size");
   if (sw.tile_bits[0] != 0) return fail(MQ_EINVAL, "tile must contain index bit 0");
   if ((int)sw.ops.size() > kMaxOps || (int)sw.phases.size() > kMaxPhases) return fail(MQ_EINVAL, "tile plan too large");
-  if (epi)
+  if (epi && (epi->perm || epi->diag))
     for (int k = 0; k < m; ++k)
       if (sw.tile_bits[k] != k) return fail(MQ_EINVAL, "fused epilogue needs the low tile [0, m)");
   const bool qft = !sw.ops.empty() && (sw.ops[0].kind == OP_QFT_FWD || sw.ops[0].kind == OP_QFT_INV);
@@ -807,6 +906,9 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
       if (D.active & (1u << k)) return fail(MQ_EINVAL, "two gates on one register slot");
       D.active |= (uint8_t)(1u << k);
       if (sw.mats_dev && sw.ops[o].kind == OP_U2) P.mat_q[op_phase[o]][k] = (int16_t)(sw.ops[o].qubit + 1);
+      else if (sw.ops[o].kind == OP_U2 && sw.ops[o].u[1] == 0.0 && sw.ops[o].u[3] == 0.0 && sw.ops[o].u[5] == 0.0 &&
+               sw.ops[o].u[7] == 0.0)
+        D.real |= (uint8_t)(1u << k);
       D.cmask[k] = sw.ops[o].kind == OP_CU2 ? sw.ops[o].cmask : 0u;
       if (D.cmask[k]) D.any_ctl = 1;
       for (int j = 0; j < 8; ++j) {
@@ -948,6 +1050,118 @@ int launch_u2_layer(mq_state* h, const double* mats, const uint8_t* active) {
 // onto itself (CNOT ladders do).  A diagonal that does not factor into
 // contiguous windows, or a permutation that mixes the low bits with high
 // ones, runs as its own pass after the sweep.
+// U = e^{i alpha} RZ(phi) RY(theta) RZ(lam) for a 2x2 unitary u (8 doubles).
+static void zyz(const double* u, double& alpha, double& phi, double& theta, double& lam) {
+  const std::complex<double> u00(u[0], u[1]), u01(u[2], u[3]), u10(u[4], u[5]), u11(u[6], u[7]);
+  alpha = 0.5 * std::arg(u00 * u11 - u01 * u10);
+  const std::complex<double> ph = std::polar(1.0, -alpha);
+  const std::complex<double> x = u00 * ph, y = u10 * ph;  // V = e^{-i alpha} U in SU(2)
+  theta = 2.0 * std::atan2(std::abs(y), std::abs(x));
+  const double pa = std::abs(x) > 1e-300 ? std::arg(x) : 0.0;
+  const double pb = std::abs(y) > 1e-300 ? std::arg(y) : 0.0;
+  phi = pb - pa;
+  lam = -pa - pb;
+}
+
+
+// launch_layer with every qubit's U(2) split as e^{i alpha} RZ(phi) RY(theta)
+// (measured at 30 qubits: fused config layer 20.7 ms against 21.7 ms with
+// complex 2x2 sweeps)
+// RZ(lam): the sweeps apply only the real RY matrices (half the arithmetic of
+// a complex 2x2), the product of all RZ(lam) is a diagonal applied in the
+// first register phase of the first sweep (before any RY), and the product of
+// all RZ(phi), the global phase and the layer's own diagonal terms ride on the
+// last register phase of the low sweep.  Sets *done = false (nothing
+// launched) when a diagonal does not fit the register-phase tables.
+static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, const int32_t* kinds,
+                              const int32_t* wires, const double* params, const uint32_t* cols, uint32_t c,
+                              bool* done) {
+  *done = false;
+  const int n = h->n;
+  std::vector<double> ry((size_t)n * 8, 0.0);
+  std::vector<int32_t> pre_k, pre_w, post_k(kinds, kinds + n_terms), post_w(wires, wires + 2 * n_terms);
+  std::vector<double> pre_p, post_p(params, params + 8 * (size_t)n_terms);
+  double alpha_sum = 0.0;
+  for (int q = 0; q < n; ++q) {
+    double al, ph, th, la;
+    zyz(mats + (size_t)q * 8, al, ph, th, la);
+    const double cs = std::cos(0.5 * th), sn = std::sin(0.5 * th);
+    double* r = ry.data() + (size_t)q * 8;
+    r[0] = cs; r[2] = -sn; r[4] = sn; r[6] = cs;
+    alpha_sum += al;
+    pre_k.push_back(MQ_DIAG_RZ); pre_w.push_back(q); pre_w.push_back(-1);
+    pre_p.push_back(la); pre_p.insert(pre_p.end(), 7, 0.0);
+    post_k.push_back(MQ_DIAG_RZ); post_w.push_back(q); post_w.push_back(-1);
+    post_p.push_back(ph); post_p.insert(post_p.end(), 7, 0.0);
+  }
+  post_k.push_back(MQ_DIAG_GLOBAL); post_w.push_back(0); post_w.push_back(-1);
+  post_p.push_back(alpha_sum); post_p.insert(post_p.end(), 7, 0.0);
+  const auto groups = split_bits(n, tile_max(h->dtype), passengers());
+  const int max_entries = kEpiLutBytes / (int)h->amp_bytes();
+  Sweep low;
+  std::vector<int> low_phase, low_rk;
+  if (!build_u2_sweep(h, ry.data(), nullptr, groups[0].first, groups[0].second, low, low_phase, low_rk)) return MQ_OK;
+  const int m = (int)low.tile_bits.size();
+  if (low.phases.empty() || low.phases.back().size() != 4 || low.phases.front().size() != 4) return MQ_OK;
+  EpiPlan e;
+  {
+    const auto& regs = low.phases.back();
+    const int rb[4] = {regs[0], regs[1], regs[2], regs[3]};
+    int rc = plan_diag_register(h, (int)post_k.size(), post_k.data(), post_w.data(), post_p.data(), rb, max_entries,
+                                e.reg);
+    if (rc) return rc;
+    if (e.reg.win.n < 0) return MQ_OK;
+    e.dreg = true;
+  }
+  // the first sweep executed carries the pre diagonal
+  Sweep first;
+  std::vector<int> first_phase, first_rk;
+  EpiPlan e_first;
+  const bool has_high = groups.size() > 1 &&
+                        build_u2_sweep(h, ry.data(), nullptr, groups[1].first, groups[1].second, first, first_phase,
+                                       first_rk);
+  {
+    const Sweep& fs = has_high ? first : low;
+    if (fs.phases.empty() || fs.phases.front().size() != 4) return MQ_OK;
+    int rb[4];
+    for (int k = 0; k < 4; ++k) rb[k] = fs.tile_bits[fs.phases.front()[k]];
+    DiagRegister& pr = has_high ? e_first.pre_reg : e.pre_reg;
+    const int budget = has_high ? max_entries : max_entries - (int)(e.reg.win.vals.size() / 2);
+    int rc = plan_diag_register(h, (int)pre_k.size(), pre_k.data(), pre_w.data(), pre_p.data(), rb, budget, pr);
+    if (rc) return rc;
+    if (pr.win.n < 0) return MQ_OK;
+    (has_high ? e_first.pre : e.pre) = true;
+  }
+  if (cols) {
+    e.perm = true;
+    for (int j = 0; j < m; ++j)
+      if (cols[j] >> m) e.perm = false;
+    if (e.perm) {
+      for (int j = 0; j < n; ++j) e.cols[j] = cols[j];
+      e.c = c;
+      int rc = ensure_alt(h);
+      if (rc) return rc;
+    }
+  }
+  *done = true;
+  for (size_t g = 1; g < groups.size(); ++g) {
+    int rc;
+    if (g == 1) {
+      rc = run_sweep(h, first, first_phase, first_rk, &e_first);
+    } else {
+      Sweep sw;
+      std::vector<int> op_phase, op_rk;
+      if (!build_u2_sweep(h, ry.data(), nullptr, groups[g].first, groups[g].second, sw, op_phase, op_rk)) continue;
+      rc = run_sweep(h, sw, op_phase, op_rk);
+    }
+    if (rc) return rc;
+  }
+  int rc = run_sweep(h, low, low_phase, low_rk, &e);
+  if (rc) return rc;
+  if (cols && !e.perm) return launch_affine_cols(h, cols, c);
+  return MQ_OK;
+}
+
 int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_terms, const int32_t* kinds,
                  const int32_t* wires, const double* params, const uint32_t* cols, uint32_t c,
                  const double* mats_dev) {
@@ -956,6 +1170,20 @@ int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_t
   if (cols) {
     uint32_t inv[32];
     if (!gf2_invert(n, cols, inv)) return fail(MQ_EINVAL, "affine map is not invertible over GF(2)");
+  }
+  // the split pays when the layer carries a diagonal of its own, which the
+  // RZ(phi) factors join at no extra cost; alone, its two diagonals cost more
+  // than the real sweeps save
+  if (mats && !mats_dev && !active && n_terms > 0 && euler_enabled(h)) {
+    // validate the layer's own terms before anything is launched
+    if (n_terms > 0) {
+      DiagWindows probe;
+      int rc = plan_diag_windows(h, n_terms, kinds, wires, params, 1, probe);
+      if (rc) return rc;
+    }
+    bool done = false;
+    int rc = launch_layer_euler(h, mats, n_terms, kinds, wires, params, cols, c, &done);
+    if (rc || done) return rc;
   }
   const auto groups = split_bits(n, tile_max(h->dtype), passengers());
   // low sweep plan first, so that argument errors surface before any launch

@@ -351,3 +351,35 @@ def test_errors_map_to_python_exceptions():
         sv.probabilities([5])
     with pytest.raises(ValueError):
         sv.apply_diag_layer if False else sv.apply_zz_weighted([(0, 0)], [0.1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
+def test_euler_split_layer_equals_complex_sweeps(dtype, monkeypatch):
+    """From 16 qubits a fused layer with a diagonal runs its U(2) gates as real
+    RY sweeps between two diagonals (the RZ factors); the result equals the
+    complex 2x2 sweeps."""
+    from mettleq_b200 import fusion as F
+    n = 19
+    rng = np.random.default_rng(77)
+    mats = np.stack([haar_u2(rng).reshape(4) for _ in range(n)])
+    terms = [(F.DIAG_ZZ, i, i + 1, [float(rng.uniform(0, math.pi))]) for i in range(n - 1)]
+    rows, c = _ladder(n)
+    vec = rand_state(n, 4, dtype)
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("MQ_EULER", flag)
+        sv = _sv(n, dtype, vec)
+        sv.apply_layer(mats, None, terms, rows, c)
+        sv.apply_u2_layer(mats)
+        out[flag] = sv.get()
+        sv.close()
+    ref = _oracle(n, np.complex128, vec)
+    for q in range(n):
+        ref.apply_single(mats[q].reshape(2, 2), q)
+    oracle_apply_terms(ref, terms)
+    ref.apply_affine(rows, c)
+    for q in range(n):
+        ref.apply_single(mats[q].reshape(2, 2), q)
+    for flag in ("1", "0"):
+        assert _err(out[flag], ref.state) <= TOL[dtype], flag
