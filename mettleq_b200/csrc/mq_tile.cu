@@ -98,6 +98,10 @@ struct TileParams {
 // over a tile and multiplied once per tile.
 constexpr int kEpiWin = 8;
 constexpr int kEpiLutBytes = 16384;
+// Register-phase diagonals first try tables of at most this many entries
+// (narrower windows, one more lookup per 16-amplitude group), which keeps
+// the sweep at the occupancy of a plain one.
+constexpr int kRegDiagSmall = 1024;
 // A diagonal applied to a 4-bit register phase: windows [0, n_win) taken at
 // the group base, times T[c][r] at lut[toff + 16c + r] (c = index bits
 // cbit[0..nc)).
@@ -1107,9 +1111,13 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
   {
     const auto& regs = low.phases.back();
     const int rb[4] = {regs[0], regs[1], regs[2], regs[3]};
-    int rc = plan_diag_register(h, (int)post_k.size(), post_k.data(), post_w.data(), post_p.data(), rb, max_entries,
-                                e.reg);
-    if (rc) return rc;
+    // small tables first: they share the SM's shared memory with the tile
+    for (int budget : {kRegDiagSmall, max_entries}) {
+      int rc = plan_diag_register(h, (int)post_k.size(), post_k.data(), post_w.data(), post_p.data(), rb, budget,
+                                  e.reg);
+      if (rc) return rc;
+      if (e.reg.win.n >= 0) break;
+    }
     if (e.reg.win.n < 0) return MQ_OK;
     e.dreg = true;
   }
@@ -1126,9 +1134,12 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
     int rb[4];
     for (int k = 0; k < 4; ++k) rb[k] = fs.tile_bits[fs.phases.front()[k]];
     DiagRegister& pr = has_high ? e_first.pre_reg : e.pre_reg;
-    const int budget = has_high ? max_entries : max_entries - (int)(e.reg.win.vals.size() / 2);
-    int rc = plan_diag_register(h, (int)pre_k.size(), pre_k.data(), pre_w.data(), pre_p.data(), rb, budget, pr);
-    if (rc) return rc;
+    const int room = has_high ? max_entries : max_entries - (int)(e.reg.win.vals.size() / 2);
+    for (int budget : {std::min(room, kRegDiagSmall / 2), room}) {
+      int rc = plan_diag_register(h, (int)pre_k.size(), pre_k.data(), pre_w.data(), pre_p.data(), rb, budget, pr);
+      if (rc) return rc;
+      if (pr.win.n >= 0) break;
+    }
     if (pr.win.n < 0) return MQ_OK;
     (has_high ? e_first.pre : e.pre) = true;
   }
@@ -1200,8 +1211,11 @@ int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_t
     if (low_u2 && !low.phases.empty() && low.phases.back().size() == 4 && m >= 4) {
       const auto& regs = low.phases.back();
       const int rb[4] = {regs[0], regs[1], regs[2], regs[3]};
-      int rc = plan_diag_register(h, n_terms, kinds, wires, params, rb, max_entries, e.reg);
-      if (rc) return rc;
+      for (int budget : {kRegDiagSmall, max_entries}) {
+        int rc = plan_diag_register(h, n_terms, kinds, wires, params, rb, budget, e.reg);
+        if (rc) return rc;
+        if (e.reg.win.n >= 0) break;
+      }
       e.dreg = e.reg.win.n >= 0;
     }
     if (!e.dreg) {
