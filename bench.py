@@ -383,11 +383,8 @@ def run_batch(args):
     for _ in range(max(0, args.warmup - 1)):
         b.run(packed=packed)
     b.synchronize()
-    stream = torch.cuda.Stream()
 
     def timed():
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
         ts = []
         for _ in range(args.steps):
             t0 = time.perf_counter()

@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "mq_internal.cuh"
@@ -354,11 +355,18 @@ template <typename R, int M, int LR, int LT>
 static int launch_adj_t(mq_state* psi, mq_state* lam, const AdjParams& P, double* partials, uint32_t* grid_out) {
   auto kern = k_adj<R, M, LR, LT>;
   const size_t smem = 4 * sizeof(V2<R>) * (size_t(1) << M);
-  static int configured = -1, bps = 0;
-  if ((int)smem > configured) {
-    MQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
-    configured = (int)std::max<size_t>(smem, 48 * 1024);
-    MQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 1 << LT, smem));
+  // one shared-memory size per instance: configure it once
+  static std::mutex mu;
+  static int configured = -1, bps_cached = 0;
+  int bps = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)smem > configured) {
+      MQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
+      configured = (int)std::max<size_t>(smem, 48 * 1024);
+      MQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps_cached, kern, 1 << LT, smem));
+    }
+    bps = bps_cached;
   }
   const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(P.n_tiles, (uint64_t)psi->num_sms * std::max(1, bps)));
   kern<<<grid, 1 << LT, smem, psi->stream>>>(reinterpret_cast<V2<R>*>(psi->cur_buf()),

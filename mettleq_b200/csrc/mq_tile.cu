@@ -140,6 +140,12 @@ struct QftParams : TileParams {
 static_assert(sizeof(QftParams) <= 32000, "kernel parameter block too large");
 static_assert(sizeof(FusedParams) <= 32000, "kernel parameter block too large");
 
+// Twiddle tables of the complex64 QFT sweeps: entry j of table w (j < 1024)
+// is e^{i pi j 2^{-10(w+1)}}.  One copy per device in global memory (read
+// through L1), uploaded by the first QFT sweep on the device; keeping them
+// out of shared memory leaves the sweep at the occupancy of a U(2) sweep.
+__device__ float2 g_qft_twiddles[3072];
+
 // e^{i pi L / 2^width}, 1 <= width <= 31, L < 2^width.
 template <typename R> struct Twiddle;
 template <> struct Twiddle<float> {
@@ -302,34 +308,35 @@ __device__ __forceinline__ V2<R> epi_phase(const EpiDesc& D, const V2<R>* lut, u
 template <typename R, int M, int LT, int CPT>
 __device__ __forceinline__ void epilogue_store(const EpiDesc& D, const V2<R>* cur, const uint32_t* cols,
                                                const V2<R>* lut, V2<R>* dst, uint32_t bo, uint32_t ib, uint32_t cl,
-                                               int tid) {
+                                               int tid, const uint32_t (&ak)[CPT]) {
   using T = V2<R>;
   constexpr int NT = 1 << LT;
   constexpr int CB = sizeof(T) == 8 ? 1 : 0;
-  constexpr int LCH = (M - CB) - LT;
   const bool perm = D.perm, diag = D.diag;
-  uint32_t at = 0;
-  if (perm) {
-#pragma unroll
-    for (int b = 0; b < LT; ++b)
-      if ((tid >> b) & 1) at ^= cols[CB + b];
-  }
   T hc = mk<R>(1, 0);
   if (diag) {
     for (int w = D.n_var; w < D.n_win; ++w)
       hc = cmul(hc, lut[D.off[w] + ((ib >> D.shift[w]) & ((1u << D.nbits[w]) - 1u))]);
   }
+  // a permutation that keeps index bit 0 (A e_0 = e_0, CNOT ladders) moves
+  // amplitude pairs: the output pair (y, y|1) is one 16-byte chunk of the
+  // input, swapped when l0 is odd
+  if constexpr (CB == 1) {
+    if (perm && !diag && cols[0] == 1u) {
+#pragma unroll
+      for (int k = 0; k < CPT; ++k) {
+        const uint32_t y = ((uint32_t)tid + (uint32_t)(k * NT)) << 1;
+        const uint32_t l0 = cl ^ ak[k];
+        const float4 v = *reinterpret_cast<const float4*>(cur + amp_slot<R>(l0 & ~1u));
+        *reinterpret_cast<float4*>(dst + (bo | y)) = (l0 & 1u) ? make_float4(v.z, v.w, v.x, v.y) : v;
+      }
+      return;
+    }
+  }
 #pragma unroll
   for (int k = 0; k < CPT; ++k) {
     const uint32_t y = ((uint32_t)tid + (uint32_t)(k * NT)) << CB;
-    uint32_t l0 = y;
-    if (perm) {
-      uint32_t ak = 0;
-#pragma unroll
-      for (int b = 0; b < LCH; ++b)
-        if ((k >> b) & 1) ak ^= cols[CB + LT + b];
-      l0 = cl ^ at ^ ak;
-    }
+    const uint32_t l0 = perm ? (cl ^ ak[k]) : y;
     T v0 = cur[amp_slot<R>(l0)];
     if (diag) v0 = cmul(v0, epi_phase<R>(D, lut, ib | l0, hc));
     if constexpr (CB == 1) {
@@ -385,13 +392,16 @@ __device__ __forceinline__ uint32_t tile_base_of(uint32_t tile, const TileParams
 // the 16 threads of a half-warp 128 bytes apart, all in one bank pair.
 //
 // MODE 0: U(2) / controlled U(2) phases; MODE 1: QFT stages; MODE 2: U(2)
-// phases plus the fused-layer epilogue (PT = FusedParams, tile bits [0, M)).
+// phases plus the fused-layer epilogue (PT = FusedParams; a permuted or
+// window-diagonal write-back needs the tile bits [0, M)); MODE 3: U(2) phases
+// with register-phase diagonals only and the plain write-back.
 template <typename R, int M, int LR, int LT, int MODE, typename PT>
-__global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? (MODE == 2 ? 2 : 3) : (LT >= 7 ? (sizeof(R) == 4 && LR == 4 ? 6 : 3) : (LT >= 6 && sizeof(R) == 4 ? 8 : 1)))))
+__global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? (MODE >= 2 ? 2 : 3) : (LT >= 7 ? (sizeof(R) == 4 && LR == 4 ? 6 : 3) : (LT >= 6 && sizeof(R) == 4 ? 8 : 1)))))
 k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   using T = V2<R>;
   constexpr bool QFT = MODE == 1;
-  constexpr bool EPI = MODE == 2;
+  constexpr bool EPI = MODE >= 2;
+  constexpr bool STORE_EPI = MODE == 2;  // MODE 3: register diagonals only, plain write-back
   constexpr int NT = 1 << LT;
   constexpr int NR = 1 << LR;
   constexpr int E = 1 << M;
@@ -404,7 +414,7 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* bufs = reinterpret_cast<T*>(smem_raw);
   PhaseDesc* phs = reinterpret_cast<PhaseDesc*>(smem_raw + 2 * sizeof(T) * E);
-  float2* tw = reinterpret_cast<float2*>(smem_raw + 2 * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases);
+  const float2* tw = nullptr;
   // MODE 2: permutation columns, then the diagonal tables
   uint32_t* ecols = reinterpret_cast<uint32_t*>(smem_raw + 2 * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases);
   T* elut = reinterpret_cast<T*>(smem_raw + 2 * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases + 128);
@@ -438,14 +448,26 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   }
   __syncthreads();
 
-  if (QFT && P.need_tw) {
-    for (int j = tid; j < 3072; j += NT) {
-      const int which = j >> 10;
-      const float x = (float)(j & 1023);
-      const float arg = x * (which == 0 ? 0x1p-10f : (which == 1 ? 0x1p-20f : 0x1p-30f));
-      float s, c;
-      sincospif(arg, &s, &c);
-      tw[j] = make_float2(c, s);
+  if constexpr (QFT) tw = g_qft_twiddles;
+  // MODE 2 with a permutation: A applied to the low offsets of this thread's
+  // output chunks (c = tid + k*NT -> amplitude c << CB), computed once
+  uint32_t epi_ak[STORE_EPI ? CPT : 1];
+#pragma unroll
+  for (int k = 0; k < (STORE_EPI ? CPT : 1); ++k) epi_ak[k] = 0;
+  if constexpr (STORE_EPI) {
+    if (P.epi.perm) {
+      uint32_t at = 0;
+#pragma unroll
+      for (int b = 0; b < LT; ++b)
+        if ((tid >> b) & 1) at ^= ecols[CB + b];
+#pragma unroll
+      for (int k = 0; k < CPT; ++k) {
+        uint32_t a = at;
+#pragma unroll
+        for (int b = 0; b < LCH; ++b)
+          if ((k >> b) & 1) a ^= ecols[CB + LT + b];
+        epi_ak[k] = a;
+      }
     }
   }
 
@@ -477,7 +499,7 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   // (returned in cl) because A maps the low space onto itself.
   auto src_base = [&](uint32_t t, uint32_t& cl) -> uint32_t {
     cl = 0;
-    if constexpr (EPI) {
+    if constexpr (STORE_EPI) {
       if (!P.epi.perm) return tile_base_of<M>(t, P);
       const uint32_t bo = t << M;
       uint32_t b = P.epi.c;
@@ -498,7 +520,6 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
     for (int k = 0; k < CPT; ++k) cp_async<16>(sb + 16u * slot(k), src + (gb | g_k(k)));
   }
   cp_async_commit();
-  if (QFT && P.need_tw) __syncthreads();
   T a[NR];
   for (int it = 0; tile < P.n_tiles; tile += gridDim.x, ++it) {
     T* cur = bufs + (it & 1) * E;
@@ -585,9 +606,9 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
       }
       __syncthreads();
     }
-    if constexpr (EPI) {
+    if constexpr (STORE_EPI) {
       if (P.epi.perm || P.epi.diag) {
-        epilogue_store<R, M, LT, CPT>(P.epi, cur, ecols, elut, dst, tile << M, base, cl_in, tid);
+        epilogue_store<R, M, LT, CPT>(P.epi, cur, ecols, elut, dst, tile << M, base, cl_in, tid, epi_ak);
         __syncthreads();
         continue;
       }
@@ -740,7 +761,7 @@ static int dispatch_tile_lr(mq_state* h, const PT& P, size_t smem, bool oop) {
 
 template <typename R, int MODE, typename PT>
 static int dispatch_tile(mq_state* h, const PT& P, size_t smem, bool oop) {
-  if constexpr (MODE == 2) {
+  if constexpr (MODE >= 2) {
     return dispatch_tile_lr<R, MODE, 4>(h, P, smem, oop);
   } else {
     if constexpr (sizeof(R) == 4) {
@@ -749,6 +770,28 @@ static int dispatch_tile(mq_state* h, const PT& P, size_t smem, bool oop) {
     }
     return dispatch_tile_lr<R, MODE, 4>(h, P, smem, oop);
   }
+}
+
+// Uploads g_qft_twiddles to the handle's device once (values formed in double
+// on the host) and waits for the copy, so every stream of the device may read
+// the table afterwards.
+static int ensure_qft_twiddles(mq_state* h) {
+  static std::mutex mu;
+  static bool done[64] = {};
+  if (h->device < 0 || h->device >= 64) return fail(MQ_EUNSUPPORTED, "device ordinal beyond 63");
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[h->device]) return MQ_OK;
+  std::vector<float2> t(3072);
+  for (int w = 0; w < 3; ++w)
+    for (int j = 0; j < 1024; ++j) {
+      const double a = M_PI * std::ldexp((double)j, -10 * (w + 1));
+      t[w * 1024 + j] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+  MQ_CUDA(cudaMemcpyToSymbolAsync(g_qft_twiddles, t.data(), t.size() * sizeof(float2), 0, cudaMemcpyHostToDevice,
+                                  h->stream));
+  MQ_CUDA(cudaStreamSynchronize(h->stream));
+  done[h->device] = true;
+  return MQ_OK;
 }
 
 // Fused-layer epilogue of a low sweep (see EpiDesc).
@@ -926,14 +969,21 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
   P.has_scale = sw.has_scale ? 1 : 0;
   P.scale = sw.has_scale ? sw.scale : 1.0;
   size_t smem = 2 * (h->amp_bytes() << m) + sizeof(PhaseDesc) * kMaxPhases;
-  if (P.need_tw) smem += 3072 * sizeof(float2);
+  if (P.need_tw) {
+    int rc = ensure_qft_twiddles(h);
+    if (rc) return rc;
+  }
   if (epi) {
     if (qft) return fail(MQ_EINVAL, "fused epilogue on a QFT sweep");
     if (h->dtype == MQ_C64) fill_epi<float>(F.epi, *epi, m, h->n);
     else fill_epi<double>(F.epi, *epi, m, h->n);
     smem += 128 + (size_t)F.epi.n_entries * h->amp_bytes();
-    if (h->dtype == MQ_C64) return dispatch_tile<float, 2>(h, F, smem, epi->perm);
-    return dispatch_tile<double, 2>(h, F, smem, epi->perm);
+    if (epi->perm || epi->diag) {
+      if (h->dtype == MQ_C64) return dispatch_tile<float, 2>(h, F, smem, epi->perm);
+      return dispatch_tile<double, 2>(h, F, smem, epi->perm);
+    }
+    if (h->dtype == MQ_C64) return dispatch_tile<float, 3>(h, F, smem, false);
+    return dispatch_tile<double, 3>(h, F, smem, false);
   }
   if (qft) {
     QftParams Q;
