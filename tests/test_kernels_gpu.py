@@ -270,7 +270,7 @@ def _ladder(n):
 
 
 @pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
-@pytest.mark.parametrize("n", [3, 5, 12, 13, 17, 22])
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 12, 13, 17, 22])
 def test_fused_config_layer(n, dtype):
     """U(2) on every qubit + RZZ chain + CNOT ladder in one apply_layer call
     (diagonal and ladder on the last U(2) sweep) equals the three layers."""
