@@ -449,6 +449,24 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   __syncthreads();
 
   if constexpr (QFT) tw = g_qft_twiddles;
+  // MODE 2 with a permutation: A (t << M) for tile index t as three 8-bit
+  // lookup tables (A is linear: the XOR of the columns of t's set bits)
+  uint32_t* htab = reinterpret_cast<uint32_t*>(elut);
+  if constexpr (STORE_EPI) {
+    htab = reinterpret_cast<uint32_t*>(elut + ((P.epi.n_entries + 1u) & ~1u));
+    if (P.epi.perm) {
+      for (int e = tid; e < 768; e += NT) {
+        const int k = e >> 8, x = e & 255;
+        uint32_t v = 0;
+        for (int bit = 0; bit < 8; ++bit) {
+          const int j = M + 8 * k + bit;
+          if (((x >> bit) & 1) && j < (int)P.n) v ^= ecols[j];
+        }
+        htab[e] = v;
+      }
+      __syncthreads();
+    }
+  }
   // MODE 2 with a permutation: A applied to the low offsets of this thread's
   // output chunks (c = tid + k*NT -> amplitude c << CB), computed once
   uint32_t epi_ak[STORE_EPI ? CPT : 1];
@@ -501,10 +519,7 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
     cl = 0;
     if constexpr (STORE_EPI) {
       if (!P.epi.perm) return tile_base_of<M>(t, P);
-      const uint32_t bo = t << M;
-      uint32_t b = P.epi.c;
-      for (int j = M; j < (int)P.n; ++j)
-        if ((bo >> j) & 1u) b ^= ecols[j];
+      const uint32_t b = P.epi.c ^ htab[t & 255u] ^ htab[256 + ((t >> 8) & 255u)] ^ htab[512 + ((t >> 16) & 255u)];
       cl = b & (uint32_t)(E - 1);
       return b & ~(uint32_t)(E - 1);
     } else {
@@ -977,7 +992,7 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
     if (qft) return fail(MQ_EINVAL, "fused epilogue on a QFT sweep");
     if (h->dtype == MQ_C64) fill_epi<float>(F.epi, *epi, m, h->n);
     else fill_epi<double>(F.epi, *epi, m, h->n);
-    smem += 128 + (size_t)F.epi.n_entries * h->amp_bytes();
+    smem += 128 + (size_t)((F.epi.n_entries + 1u) & ~1u) * h->amp_bytes() + (F.epi.perm ? 768 * 4 : 0);
     if (epi->perm || epi->diag) {
       if (h->dtype == MQ_C64) return dispatch_tile<float, 2>(h, F, smem, epi->perm);
       return dispatch_tile<double, 2>(h, F, smem, epi->perm);
