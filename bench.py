@@ -491,7 +491,7 @@ def run_serve(args):
     """Poisson stream at 200 requests/s, n log-uniform in [12, 30], depth
     U{10..100} config-0 layers (QFT and GF(2) layer each with p = 0.1), 1000
     shots, complex64, 150 GB admission budget; beside it the plain path (one
-    request at a time through Device.execute) on the first requests."""
+    request at a time through Device.execute) on the same request stream."""
     from mettleq_b200.serving import Server, poisson_requests, serve_plain
     count = args.count or 200
     reqs = poisson_requests(count, rate=200.0, seed=args.seed)
@@ -500,8 +500,7 @@ def run_serve(args):
     stats, clk = _timed_clocks(lambda: srv.serve(reqs, realtime=True))
     peak, active = srv.peak_used, srv.peak_active
     srv.close()
-    plain_n = max(1, count // 5)
-    plain = serve_plain(poisson_requests(count, rate=200.0, seed=args.seed)[:plain_n], realtime=True)
+    plain = serve_plain(poisson_requests(count, rate=200.0, seed=args.seed), realtime=True)
     return {
         "metric": "serve p50 latency", "value": stats["p50_s"], "unit": "s", "n_gpus": 1, "steps": 1,
         "warmup": 1, "ms_per_step": stats["makespan_s"] * 1e3, "higher_is_better": False, "scaling": "weak",

@@ -72,6 +72,10 @@ int mq_state_info(const mq_state* h, int* n, int* dtype, int* device);
 int mq_state_set_stream(mq_state* h, void* stream);
 /* The stream the handle launches on (its own or the caller's). */
 int mq_state_stream(const mq_state* h, void** out);
+/* Size this handle's launch grids for at most `sms` SMs (<= 0: all), so that
+ * kernels of other streams find free SMs while its kernels run (a serving
+ * loop keeps a reserve for short requests this way). */
+int mq_state_set_sm_limit(mq_state* h, int sms);
 int mq_state_reset(mq_state* h);                       /* sim.py:32-45 */
 int mq_state_set(mq_state* h, const void* host_amps);  /* 2^n amplitudes */
 int mq_state_get(mq_state* h, void* host_amps);
@@ -121,7 +125,9 @@ int mq_apply_layer(mq_state* h, const double* mats, const uint8_t* active,
 
 /* ---- (c) QFT (shaders/qft.py:144-236, sim.py:522-563) -------------------- */
 /* Ordered wire list, first wire = most significant logical bit, no final
- * swaps; inverse != 0 applies iqft. */
+ * swaps; inverse != 0 applies iqft.  The first complex64 QFT sweep on a
+ * device uploads the library's twiddle table and waits for that copy (once
+ * per device and process): make it before any stream capture. */
 int mq_apply_qft(mq_state* h, const int32_t* wires, int k, int inverse);
 /* Stages [j_begin, j_end) of the QFT on qubits [q0, q0+k): the fused stage
  * passes of qft_stage_sub (qft.py:144-181); j_begin=0, j_end=k is the full

@@ -36,6 +36,7 @@ SIGNATURES = {
     "mq_state_info": (_I, [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
     "mq_state_set_stream": (_I, [_P, _P]),
     "mq_state_stream": (_I, [_P, C.POINTER(_P)]),
+    "mq_state_set_sm_limit": (_I, [_P, _I]),
     "mq_state_reset": (_I, [_P]),
     "mq_state_set": (_I, [_P, _P]),
     "mq_state_get": (_I, [_P, _P]),

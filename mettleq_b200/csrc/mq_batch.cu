@@ -239,6 +239,7 @@ static int lane_state_for(mq_batch* b, int lane, int n, mq_state** out) {
   h->dtype = MQ_C64;
   h->device = b->device;
   h->num_sms = b->num_sms;
+  h->device_sms = b->num_sms;
   h->stream = b->lane_stream[lane];
   h->state_bytes = (size_t(1) << n) * 8;
   cudaError_t e = cudaMalloc(&h->buf[0], h->state_bytes);

@@ -126,7 +126,10 @@ int mq_state_create(int n, int dtype, int device, void* stream, mq_state** out) 
   h->device = device;
   h->state_bytes = (size_t)bytes;
   int sms = 0;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0) h->num_sms = sms;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0) {
+    h->num_sms = sms;
+    h->device_sms = sms;
+  }
   if (stream) {
     h->stream = (cudaStream_t)stream;
   } else {
@@ -180,6 +183,12 @@ int mq_state_set_stream(mq_state* h, void* stream) {
     MQ_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
   }
+  return MQ_OK;
+}
+
+int mq_state_set_sm_limit(mq_state* h, int sms) {
+  MQ_CHECK_HANDLE(h);
+  h->num_sms = (sms <= 0 || sms > h->device_sms) ? h->device_sms : sms;
   return MQ_OK;
 }
 

@@ -330,7 +330,7 @@ int plan_diag_windows(mq_state* h, int n_terms, const int32_t* kinds, const int3
 }
 
 // The diagonal split for a register phase whose register bits are rbits[4]
-// (ascending): phase(x) = W(x) * T[c(x)][r(x)] with r(x) the four register
+// (ascending): phase(x) = W(x) * T[c(x)][r(x)] (row c at entry 17c) with r(x) the four register
 // bits, c(x) the values of the (at most 3) other bits that share a term with
 // a register bit, T the product of those terms, and W the remaining terms as
 // contiguous windows that do not read the register bits (so W can be taken
@@ -368,7 +368,7 @@ int plan_diag_register(mq_state* h, int n_terms, const int32_t* kinds, const int
   bool ok = false;
   for (int W = 10; W >= 1 && !ok; --W) {
     luts = plan_luts(group, W);
-    size_t entries = nt;
+    size_t entries = (nt / 16) * 17;
     bool contig = true;
     for (auto& L : luts) {
       entries += L.vals.size();
@@ -391,10 +391,16 @@ int plan_diag_register(mq_state* h, int n_terms, const int32_t* kinds, const int
     }
     off += (uint32_t)luts[l].vals.size();
   }
+  // rows of 16 at a stride of 17 entries: lanes that read rows c and c' of
+  // the same register pattern hit different shared-memory banks
   out.t_off = (int)off;
-  for (auto v : T) {
-    out.win.vals.push_back(v.real());
-    out.win.vals.push_back(v.imag());
+  for (uint32_t c = 0; c < nt / 16; ++c) {
+    for (uint32_t r = 0; r < 16; ++r) {
+      out.win.vals.push_back(T[c * 16 + r].real());
+      out.win.vals.push_back(T[c * 16 + r].imag());
+    }
+    out.win.vals.push_back(1.0);
+    out.win.vals.push_back(0.0);
   }
   return MQ_OK;
 }

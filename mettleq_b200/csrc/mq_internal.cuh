@@ -74,7 +74,8 @@ struct mq_state {
   int n = 0;
   int dtype = MQ_C64;
   int device = 0;
-  int num_sms = 148;
+  int num_sms = 148;         // SMs the launch grids are sized for (mq_state_set_sm_limit)
+  int device_sms = 148;      // SMs of the device
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   void* buf[2] = {nullptr, nullptr};
@@ -129,7 +130,7 @@ int plan_diag_windows(mq_state* h, int n_terms, const int32_t* kinds, const int3
                       int max_entries, DiagWindows& out);
 // A diagonal factored for a 4-bit register phase (plan_diag_register):
 // window tables (win, evaluated at the register group's base) followed, at
-// entry t_off, by T[c][r] (16 << nc entries) indexed by the register bits r
+// entry t_off, by T[c][r] (row c at t_off + 17c, 17 << nc entries) indexed by the register bits r
 // and the cross bits c = bits cbit[0..nc) of the index.
 struct DiagRegister {
   DiagWindows win;

@@ -103,8 +103,8 @@ constexpr int kEpiLutBytes = 16384;
 // the sweep at the occupancy of a plain one.
 constexpr int kRegDiagSmall = 1024;
 // A diagonal applied to a 4-bit register phase: windows [0, n_win) taken at
-// the group base, times T[c][r] at lut[toff + 16c + r] (c = index bits
-// cbit[0..nc)).
+// the group base, times T[c][r] at lut[toff + 17c + r] (c = index bits
+// cbit[0..nc); rows padded to 17 entries against bank conflicts).
 struct RegDiag {
   uint8_t on, nc, cbit[3], n_win, pad[2];
   uint8_t shift[kEpiWin];
@@ -116,7 +116,7 @@ struct EpiDesc {
   RegDiag pre;  // applied in the first register phase, before its gates
   uint8_t diag, perm, n_win, n_var;
   // dreg: the diagonal is applied in the last register phase instead:
-  // windows [0, n_win) at the group base times T[c][r] at lut[toff + 16c + r]
+  // windows [0, n_win) at the group base times T[c][r] at lut[toff + 17c + r]
   // (c = index bits cbit[0..nc))
   uint8_t dreg, nc, cbit[3], pad0;
   uint16_t toff, pad1;
@@ -363,7 +363,7 @@ __device__ __forceinline__ void apply_regdiag(V2<R> (&a)[16], const V2<R>* lut, 
 #pragma unroll
   for (int j = 0; j < 3; ++j)
     if (j < D.nc) cc |= ((gq >> D.cbit[j]) & 1u) << j;
-  const T* tr = lut + D.toff + (cc << 4);
+  const T* tr = lut + D.toff + cc * 17u;
 #pragma unroll
   for (int r = 0; r < 16; ++r) a[r] = cmul(a[r], cmul(f, tr[r]));
 }
@@ -396,7 +396,7 @@ __device__ __forceinline__ uint32_t tile_base_of(uint32_t tile, const TileParams
 // window-diagonal write-back needs the tile bits [0, M)); MODE 3: U(2) phases
 // with register-phase diagonals only and the plain write-back.
 template <typename R, int M, int LR, int LT, int MODE, typename PT>
-__global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? (MODE >= 2 ? 2 : 3) : (LT >= 7 ? (sizeof(R) == 4 && LR == 4 ? 6 : 3) : (LT >= 6 && sizeof(R) == 4 ? 8 : 1)))))
+__global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? (MODE == 2 ? 2 : 3) : (LT >= 7 ? (sizeof(R) == 4 && LR == 4 ? 6 : 3) : (LT >= 6 && sizeof(R) == 4 ? 8 : 1)))))
 k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   using T = V2<R>;
   constexpr bool QFT = MODE == 1;
@@ -604,7 +604,7 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
 #pragma unroll
             for (int j = 0; j < 3; ++j)
               if (j < P.epi.nc) cc |= ((gq >> P.epi.cbit[j]) & 1u) << j;
-            const T* tr = elut + P.epi.toff + (cc << 4);
+            const T* tr = elut + P.epi.toff + cc * 17u;
 #pragma unroll
             for (int r = 0; r < NR; ++r) a[r] = cmul(a[r], cmul(f, tr[r]));
           }
@@ -681,7 +681,7 @@ static int passengers() { return env_int("MQ_TILE_PASSENGERS", 4, 0, 5); }
 static bool euler_enabled(const mq_state* h) {
   const char* v = std::getenv("MQ_EULER");
   if (v && v[0] == '0') return false;
-  return h->n >= env_int("MQ_EULER_MIN_QUBITS", 16, 1, 32);
+  return h->n >= env_int("MQ_EULER_MIN_QUBITS", 20, 1, 32);
 }
 static int min_tile() { return env_int("MQ_TILE_MIN", 10, 1, 12); }
 

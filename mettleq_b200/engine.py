@@ -144,6 +144,10 @@ class StateVector:
         N.check(self._lib.mq_state_stream(self._h, C.byref(out)))
         return int(out.value or 0)
 
+    def set_sm_limit(self, sms: int) -> None:
+        """Launch grids for at most ``sms`` SMs (<= 0: all of them)."""
+        N.check(self._lib.mq_state_set_sm_limit(self._h, int(sms)))
+
     def set_stream(self, stream: Optional[int]) -> None:
         N.check(self._lib.mq_state_set_stream(self._h, C.c_void_p(stream or 0)))
 
@@ -252,14 +256,11 @@ class StateVector:
         N.check(self._lib.mq_apply_xor_affine(self._h, _ptr(r), int(c)))
 
     # -- fused layer ----------------------------------------------------------
-    def apply_layer(self, mats=None, active: Optional[Iterable[int]] = None,
-                    terms: Sequence[Tuple[int, int, int, Sequence[float]]] = (),
-                    rows: Optional[Sequence[int]] = None, c: int = 0) -> None:
-        """U(2) on the active qubits, then the commuting diagonal ``terms``,
-        then the permutation out[y] = in[f^{-1}(y)] (inverse ``rows``/``c``),
-        in the sweeps of the U(2) layer alone where the diagonal and the
-        permutation allow it (one config-0 layer: u2_list_layer_all +
-        zz_weighted_layer + xor_affine_gather, device.py:1089-1097)."""
+    def pack_layer(self, mats=None, active: Optional[Iterable[int]] = None,
+                   terms: Sequence[Tuple[int, int, int, Sequence[float]]] = (),
+                   rows: Optional[Sequence[int]] = None, c: int = 0) -> tuple:
+        """The C arrays of ``apply_layer`` (validated), for layers applied
+        more than once or issued from a latency-sensitive loop."""
         m = act = None
         if mats is not None:
             m = _mats_array(self.n, mats)
@@ -275,6 +276,11 @@ class StateVector:
             r = np.ascontiguousarray(np.asarray([int(x) for x in rows], dtype=np.uint64))
             if r.size != self.n:
                 raise ValueError("rows must have one mask per qubit")
+        return (m, act, kinds, wires, params, r, int(c))
+
+    def apply_packed_layer(self, packed: tuple) -> None:
+        """``apply_layer`` from the arrays of ``pack_layer``."""
+        m, act, kinds, wires, params, r, c = packed
         for a in (m, act, kinds, wires, params, r):
             if a is not None:
                 self.param_bytes += a.nbytes
@@ -282,7 +288,17 @@ class StateVector:
             self._h, _ptr(m) if m is not None else None, _ptr(act) if act is not None else None,
             0 if kinds is None else int(kinds.size), _ptr(kinds) if kinds is not None else None,
             _ptr(wires) if wires is not None else None, _ptr(params) if params is not None else None,
-            _ptr(r) if r is not None else None, int(c)))
+            _ptr(r) if r is not None else None, c))
+
+    def apply_layer(self, mats=None, active: Optional[Iterable[int]] = None,
+                    terms: Sequence[Tuple[int, int, int, Sequence[float]]] = (),
+                    rows: Optional[Sequence[int]] = None, c: int = 0) -> None:
+        """U(2) on the active qubits, then the commuting diagonal ``terms``,
+        then the permutation out[y] = in[f^{-1}(y)] (inverse ``rows``/``c``),
+        in the sweeps of the U(2) layer alone where the diagonal and the
+        permutation allow it (one config-0 layer: u2_list_layer_all +
+        zz_weighted_layer + xor_affine_gather, device.py:1089-1097)."""
+        self.apply_packed_layer(self.pack_layer(mats, active, terms, rows, c))
 
     # -- (e) probabilities, sampling, expectations ------------------------
     def probabilities(self, wires: Optional[Sequence[int]] = None, dtype=np.float64) -> np.ndarray:

@@ -12,10 +12,16 @@ it.  ``Server`` runs a request loop over one GPU instead:
     than ``max_bypass_s``;
   * every admitted request keeps its statevector resident on its own CUDA
     stream (higher priority for fewer qubits) for all its layers and shots;
-    each round the loop issues a few layers to the active requests with the
-    least remaining work, so short requests overtake long ones while the
-    work of several requests overlaps on the device, and polls CUDA events
-    to notice completion;
+    at most ``max_large`` requests with more than ``small_work`` amplitude-
+    layers are on the device at once, and their launch grids leave
+    ``sm_reserve`` SMs free, so short requests never wait for a sweep that
+    holds the whole GPU;
+    each round the loop issues work to the active requests with the least
+    remaining work first, within a few milliseconds of host time: a request
+    whose remaining work is small (up to 100 layers of 22 qubits) gets all
+    of it at once, larger ones a few layers per round; short requests thus
+    overtake long ones while the work of several requests overlaps on the
+    device, and the loop polls CUDA events to notice completion;
   * finished requests draw their shots (mq_sample, seeded Philox stream) and
     give their state back to a pool, so steady-state serving allocates and
     frees no device memory (a cudaFree would stall every stream).
@@ -119,9 +125,13 @@ def poisson_requests(count: int, rate: float = 200.0, seed: int = 0, n_range: Tu
 
 def apply_request_layer(sv: StateVector, L: RequestLayer, ladder) -> None:
     """One layer: fused U(2) + RZZ chain + CNOT ladder, then the optional QFT
-    and permutation."""
-    terms = [(DIAG_ZZ, i, i + 1, [float(t) / 2.0]) for i, t in enumerate(L.thetas)]
-    sv.apply_layer(L.mats, None, terms, *ladder)
+    and permutation.  The layer's C arrays are packed on first use."""
+    packed = getattr(L, "_packed", None)
+    if packed is None:
+        terms = [(DIAG_ZZ, i, i + 1, [float(t) / 2.0]) for i, t in enumerate(L.thetas)]
+        packed = sv.pack_layer(L.mats, None, terms, *ladder)
+        L._packed = packed
+    sv.apply_packed_layer(packed)
     if L.qft:
         sv.apply_qft(None)
     if L.xor is not None:
@@ -172,11 +182,16 @@ class Server:
     """Continuous-batching request loop (see the module docstring)."""
 
     def __init__(self, budget_bytes: int = 150 * 10 ** 9, max_active: int = 64, layers_per_round: int = 4,
-                 max_bypass_s: float = 30.0, device: int = 0, keep_states: bool = False, issue_width: int = 6):
+                 max_bypass_s: float = 30.0, device: int = 0, keep_states: bool = False,
+                 round_budget_s: float = 0.004, small_work: int = 100 << 22, max_large: int = 8,
+                 sm_reserve: int = 20):
         self.budget = int(budget_bytes)
         self.max_active = int(max_active)
         self.k = int(layers_per_round)
-        self.issue_width = int(issue_width)
+        self.round_budget_s = float(round_budget_s)    # host time spent issuing per round
+        self.small_work = int(small_work)              # layers x 2^n issued in one go
+        self.max_large = int(max_large)                # large requests on the device at once
+        self.sm_reserve = int(sm_reserve)              # SMs large requests leave to the others
         self.max_bypass_s = float(max_bypass_s)
         self.device = int(device)
         self.keep_states = keep_states
@@ -197,6 +212,7 @@ class Server:
         admitted / finished / samples of each request and returns summary
         statistics (latency = finished - arrival)."""
         import torch
+        self._sms = torch.cuda.get_device_properties(self.device).multi_processor_count
         for r in requests:
             if r.footprint > self.budget:
                 raise MemoryError(f"request {r.rid}: {r.n} qubits need {r.footprint} bytes, budget {self.budget}")
@@ -220,8 +236,13 @@ class Server:
                 else:
                     waiting.sort(key=lambda r: r.work)
             i = 0
+            n_large = sum(1 for a in active if a["large"])
             while i < len(waiting) and len(active) < self.max_active:
                 r = waiting[i]
+                large = r.work > self.small_work
+                if large and n_large >= self.max_large:
+                    i += 1
+                    continue
                 if used + r.footprint <= self.budget:
                     reuse = bool(self.pool.free.get(r.n))
                     if not reuse:
@@ -230,8 +251,13 @@ class Server:
                             self.pool.evict(over)
                     sv, stream = self.pool.get(r.n)
                     sv.reset()
+                    # large requests leave SMs free, so the kernels of short
+                    # requests start without waiting for a whole-GPU sweep
+                    sv.set_sm_limit(self._sms - self.sm_reserve if large else 0)
+                    n_large += 1 if large else 0
                     r.admitted = now()
-                    active.append({"req": r, "sv": sv, "stream": stream, "next": 0, "events": deque()})
+                    active.append({"req": r, "sv": sv, "stream": stream, "next": 0, "events": deque(),
+                                   "large": large})
                     used += r.footprint
                     self.peak_used = max(self.peak_used, used)
                     self.peak_active = max(self.peak_active, len(active))
@@ -240,13 +266,15 @@ class Server:
                 if i == 0 and now() - r.arrival > self.max_bypass_s:
                     break  # the overdue head waits for room; nothing passes it
                 i += 1
-            # issue: smallest remaining work first, a few requests per round,
-            # at most two chunks of layers queued per request
+            # issue: smallest remaining work first within a host-time budget
+            # per round; a request whose whole remaining work is small gets
+            # all of it at once, larger ones a chunk of layers, with at most
+            # two chunks queued per request
             progressed = False
             order = sorted(active, key=lambda a: (len(a["req"].layers) - a["next"]) << a["req"].n)
-            issued = 0
+            round_end = clock() + self.round_budget_s
             for a in order:
-                if issued >= self.issue_width:
+                if clock() > round_end:
                     break
                 r = a["req"]
                 ev = a["events"]
@@ -254,8 +282,9 @@ class Server:
                     ev.popleft()
                 if a["next"] >= len(r.layers) or len(ev) >= 2:
                     continue
-                issued += 1
-                stop = min(len(r.layers), a["next"] + self.k)
+                left = len(r.layers) - a["next"]
+                chunk = left if (left << r.n) <= self.small_work else self.k
+                stop = min(len(r.layers), a["next"] + chunk)
                 for j in range(a["next"], stop):
                     apply_request_layer(a["sv"], r.layers[j], self._ladder(r.n))
                 a["next"] = stop

@@ -356,11 +356,11 @@ def test_errors_map_to_python_exceptions():
 @pytest.mark.gpu
 @pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
 def test_euler_split_layer_equals_complex_sweeps(dtype, monkeypatch):
-    """From 16 qubits a fused layer with a diagonal runs its U(2) gates as real
+    """From 20 qubits a fused layer with a diagonal runs its U(2) gates as real
     RY sweeps between two diagonals (the RZ factors); the result equals the
     complex 2x2 sweeps."""
     from mettleq_b200 import fusion as F
-    n = 19
+    n = 21
     rng = np.random.default_rng(77)
     mats = np.stack([haar_u2(rng).reshape(4) for _ in range(n)])
     terms = [(F.DIAG_ZZ, i, i + 1, [float(rng.uniform(0, math.pi))]) for i in range(n - 1)]
@@ -383,3 +383,25 @@ def test_euler_split_layer_equals_complex_sweeps(dtype, monkeypatch):
         ref.apply_single(mats[q].reshape(2, 2), q)
     for flag in ("1", "0"):
         assert _err(out[flag], ref.state) <= TOL[dtype], flag
+
+
+@pytest.mark.gpu
+def test_device_shots_agree_with_reference_probabilities():
+    """1000 device shots from the reference's own 8-qubit state, against the
+    reference's exact probabilities (chi-square, tail pooled): the sampled
+    counts agree in distribution, as the reference's MLX stream is not
+    reproducible off Apple hardware."""
+    import os
+    from scipy.stats import chi2
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_outputs.npz"))
+    probs = np.asarray(g["probs_0_1_2_3_4_5_6_7"], dtype=np.float64)
+    probs /= probs.sum()
+    sv = _sv(8, np.complex64, np.asarray(g["layers_uniform"], dtype=np.complex64))
+    for seed in (11, 12):
+        idx = sv.sample_indices(1000, seed=seed)
+        counts = np.bincount(idx, minlength=256).astype(np.float64)
+        keep = probs * 1000 >= 5.0
+        obs = np.append(counts[keep], counts[~keep].sum())
+        exp = np.append(probs[keep] * 1000, probs[~keep].sum() * 1000)
+        stat = float(np.sum((obs - exp) ** 2 / exp))
+        assert chi2.sf(stat, obs.size - 1) > 1e-3, seed

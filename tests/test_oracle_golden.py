@@ -208,3 +208,28 @@ def test_marginal_order_first_wire_msb():
     p = S.amp2(o.state)
     m = S.marginal_probabilities(p, 3, [2, 0])
     assert np.allclose(m, [0, 1, 0, 0])
+
+
+def _chi2_pvalue(counts, probs):
+    from scipy.stats import chi2
+    shots = counts.sum()
+    keep = probs * shots >= 5.0          # pool the sparse tail into one bin
+    obs = np.append(counts[keep], counts[~keep].sum())
+    exp = np.append(probs[keep] * shots, probs[~keep].sum() * shots)
+    m = exp > 0
+    stat = float(np.sum((obs[m] - exp[m]) ** 2 / exp[m]))
+    return float(chi2.sf(stat, int(m.sum()) - 1))
+
+
+def test_sampled_counts_agree_with_reference_probabilities(ref):
+    """MLX's generator cannot run here, so counts are compared in distribution:
+    1000 shots of the project's seeded stream on the reference's own state
+    (layers_uniform) against the reference's exact probabilities (chi-square
+    over bins with >= 5 expected counts, the tail pooled)."""
+    probs = np.asarray(ref["probs_0_1_2_3_4_5_6_7"], dtype=np.float64)
+    probs = probs / probs.sum()
+    state = np.asarray(ref["layers_uniform"], dtype=np.complex128)
+    for seed in (1, 2, 3):
+        idx = S.sample_indices(S.amp2(state), seed, 1000)
+        counts = np.bincount(idx, minlength=probs.size).astype(np.float64)
+        assert _chi2_pvalue(counts, probs) > 1e-3, seed
