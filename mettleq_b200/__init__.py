@@ -1,9 +1,13 @@
 """B200-native statevector engine: a drop-in for MettleQ's method="statevector" path.
 
-Layers (see DESIGN.md at the repository root for the full map):
-  engine.StateVector   -- kernel-level API over the C ABI (libmq.so)
-  device.Device        -- op-dict runtime with gate-stream fusion (device.py)
+Layers:
+  engine.StateVector   -- kernel-level API over the C ABI (libmq.so, include/mq.h)
+  device.Device        -- op-dict runtime with gate-stream fusion (reference device.py)
   integrations._common -- SDK glue (execute_operations, sampling, Pauli sums)
+  adjoint              -- adjoint-method gradients, torch.autograd.Function
+  batch                -- many circuits in one CUDA graph
+  serving              -- continuous-batching request loop
+  replicas             -- one replica per GPU for independent units
 """
 from ._native import StatevectorMemoryError  # noqa: F401
 
