@@ -36,7 +36,7 @@ enum mq_status {
   MQ_ENOMEM = 2,      /* refused or failed allocation: StatevectorMemoryError (execution.py:33-38, 377-407) */
   MQ_EDEVICE = 3,     /* CUDA/device failure: RuntimeError (device.py:97-139) */
   MQ_ETIMEOUT = 4,    /* a bounded device wait gave up */
-  MQ_EUNSUPPORTED = 5 /* request outside what this build supports */
+  MQ_EUNSUPPORTED = 5 /* request outside what the library supports */
 };
 
 enum mq_dtype { MQ_C64 = 0, MQ_C128 = 1 };
