@@ -65,6 +65,7 @@ struct AdjParams {
   uint8_t n, m, n_phases, store_psi;
   uint8_t tile_bit[16];
   uint8_t hi_contig, hi_shift, pad[6];
+  BaseRuns runs;  // tile index -> base index (deposit_runs)
   AdjPhase ph[kAdjMaxPhases];
 };
 
@@ -176,15 +177,7 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
       if ((k >> b) & 1) g |= 1u << P.tile_bit[CB + LT + b];
     return g;
   };
-  auto base_of = [&](uint32_t tile) -> uint32_t {
-    uint64_t x = tile;
-#pragma unroll
-    for (int k = 0; k < M; ++k) {
-      const int pb = P.tile_bit[k];
-      x = ((x >> pb) << (pb + 1)) | (x & ((uint64_t(1) << pb) - 1));
-    }
-    return (uint32_t)x;
-  };
+  auto base_of = [&](uint32_t tile) -> uint32_t { return deposit_runs(tile, P.runs); };
   auto issue = [&](uint32_t tile, int which) {
     const uint32_t gb = base_of(tile) | g_t;
     const uint32_t sp = smem_u32(bufs + which * E), sl = smem_u32(bufs + (2 + which) * E);
@@ -433,6 +426,7 @@ static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
   P.m = (uint8_t)m;
   P.store_psi = store_psi ? 1 : 0;
   for (int k = 0; k < m; ++k) P.tile_bit[k] = (uint8_t)tile_bits[k];
+  make_base_runs(P.runs, n, P.tile_bit, m);
   {
     const int cb = c64 ? 1 : 0;
     const int lt = std::min(lrt == 3 ? 8 : 7, m - lr);

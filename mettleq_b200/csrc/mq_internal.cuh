@@ -50,6 +50,48 @@ constexpr int kMaxQubits = 32;        // 32-bit amplitude indices
 constexpr int kTileMaxC64 = 13;       // 2^13 complex64 = 64 KiB tile
 constexpr int kTileMaxC128 = 12;      // 2^12 complex128 = 64 KiB tile
 
+// ---------------------------------------------------------------- tile bases
+// The base index of tile t of a sweep: t's bits deposited, in ascending
+// order, into the index bits that are not tile bits.  Those free bits form
+// at most (tile bits + 1) contiguous runs; run j takes t's bits
+// [src[j], src[j] + len) (mask = 2^len - 1) to index bits [dst[j], ...).
+// One shift, mask and shift per run replaces a per-tile-bit insertion loop.
+constexpr int kMaxRuns = 14;
+struct BaseRuns {
+  uint8_t n;
+  uint8_t src[kMaxRuns];
+  uint8_t dst[kMaxRuns];
+  uint8_t pad;
+  uint32_t mask[kMaxRuns];
+};
+__host__ __device__ __forceinline__ uint32_t deposit_runs(uint32_t t, const BaseRuns& R) {
+  uint32_t x = 0;
+#pragma unroll
+  for (int j = 0; j < kMaxRuns; ++j) {
+    if (j >= R.n) break;
+    x |= ((t >> R.src[j]) & R.mask[j]) << R.dst[j];
+  }
+  return x;
+}
+// tile_bits: the m tile bits of an n-qubit index, ascending, m <= 13.
+inline void make_base_runs(BaseRuns& R, int n, const uint8_t* tile_bits, int m) {
+  R = BaseRuns{};
+  uint32_t tmask = 0;
+  for (int k = 0; k < m; ++k) tmask |= 1u << tile_bits[k];
+  int src = 0;
+  for (int b = 0; b < n;) {
+    if ((tmask >> b) & 1u) { ++b; continue; }
+    const int start = b;
+    while (b < n && !((tmask >> b) & 1u)) ++b;
+    const int len = b - start;
+    R.src[R.n] = (uint8_t)src;
+    R.dst[R.n] = (uint8_t)start;
+    R.mask[R.n] = len >= 32 ? 0xffffffffu : ((1u << len) - 1u);
+    src += len;
+    ++R.n;
+  }
+}
+
 // ---------------------------------------------------------------- errors
 void set_error(int code, const std::string& msg);
 int fail(int code, const std::string& msg);

@@ -45,6 +45,10 @@ namespace mq {
 enum : uint8_t { OP_U2 = 0, OP_QFT_FWD = 1, OP_QFT_INV = 2, OP_CU2 = 3 };
 
 constexpr int kMaxPhases = 6;
+// Tile buffers in shared memory: two (the next tile is prefetched while one
+// is processed), or one for 13-bit tiles at 256 threads, where three CTAs per
+// SM overlap one another's loads instead.
+__host__ __device__ constexpr int tile_nbuf(int m, int lt) { return (m >= 13 && lt <= 8) ? 1 : 2; }
 constexpr int kMaxOps = 16;
 constexpr int kMaxTileBits = 13;
 
@@ -67,6 +71,11 @@ struct __align__(16) PhaseDesc {
   uint8_t active;        // slots carrying a gate
   uint8_t any_ctl;       // some slot is controlled
   uint8_t real;          // slots whose matrix is real (RY-type: 2 FMA per output component)
+  // slots holding a rotation [[c, -s], [s, c]] as one tangent t in uf/ud[k][0]:
+  // c (x0 - t x1, t x0 + x1) with t = s / c, or (rotB) s (t x0 - x1, x0 + t x1)
+  // with t = c / s; the factor c or s is left to the caller (one FMA per
+  // output component)
+  uint8_t rot, rotB;
   alignas(16) float uf[5][8];   // rows read as two 16-byte vectors
   alignas(16) double ud[5][8];
 };
@@ -79,6 +88,7 @@ struct TileParams {
   uint8_t tile_bit[16];
   uint8_t need_tw, has_scale, hi_contig, hi_shift;
   uint32_t pad2;
+  BaseRuns runs;  // tile index -> base index (deposit_runs)
   double scale;
   uint8_t ph_op[kMaxPhases + 2];     // QFT: ops of phase p are [ph_op[p], ph_op[p+1])
   // U(2) matrices read from device memory at launch (mats_dev[8 q ..]):
@@ -184,7 +194,9 @@ __device__ __forceinline__ T cmac2(T u0, T x0, T u1, T x1) {
 }
 
 // 2x2 gate on register bit K; CTL: only where all cmask bits are set.
-template <typename R, int LR, int K, bool CTL>
+// REAL: real matrices take the real path (else the complex one; the sweeps
+// with register diagonals leave it out for registers).
+template <typename R, int LR, int K, bool CTL, bool REAL>
 __device__ __forceinline__ void apply_u2(V2<R> (&a)[1 << LR], const PhaseDesc& D, uint32_t gq, const uint32_t* greg) {
   using T = V2<R>;
   constexpr int NR = 1 << LR;
@@ -199,7 +211,32 @@ __device__ __forceinline__ void apply_u2(V2<R> (&a)[1 << LR], const PhaseDesc& D
     u10 = mk<R>(D.ud[K][4], D.ud[K][5]); u11 = mk<R>(D.ud[K][6], D.ud[K][7]);
   }
   const uint32_t cm = D.cmask[K];
-  if (!CTL && ((D.real >> K) & 1u)) {
+  if (!CTL && ((D.rot >> K) & 1u)) {
+    const R t = u00.x;
+    if ((D.rotB >> K) & 1u) {
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        if (r & (1 << K)) continue;
+        const T x0 = a[r], x1 = a[r | (1 << K)];
+        a[r].x = fma(t, x0.x, -x1.x);
+        a[r].y = fma(t, x0.y, -x1.y);
+        a[r | (1 << K)].x = fma(t, x1.x, x0.x);
+        a[r | (1 << K)].y = fma(t, x1.y, x0.y);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        if (r & (1 << K)) continue;
+        const T x0 = a[r], x1 = a[r | (1 << K)];
+        a[r].x = fma(-t, x1.x, x0.x);
+        a[r].y = fma(-t, x1.y, x0.y);
+        a[r | (1 << K)].x = fma(t, x0.x, x1.x);
+        a[r | (1 << K)].y = fma(t, x0.y, x1.y);
+      }
+    }
+    return;
+  }
+  if (REAL && !CTL && ((D.real >> K) & 1u)) {
     // real matrix: each output component is two products
     const R c00 = u00.x, c01 = u01.x, c10 = u10.x, c11 = u11.x;
 #pragma unroll
@@ -223,15 +260,15 @@ __device__ __forceinline__ void apply_u2(V2<R> (&a)[1 << LR], const PhaseDesc& D
   }
 }
 
-template <typename R, int LR, bool CTL>
+template <typename R, int LR, bool CTL, bool REAL>
 __device__ __forceinline__ void apply_u2_phase(V2<R> (&a)[1 << LR], const PhaseDesc& D, uint32_t gq,
                                                const uint32_t* greg) {
   const uint32_t act = D.active;
-  if (act & 1u) apply_u2<R, LR, 0, CTL>(a, D, gq, greg);
-  if constexpr (LR > 1) if (act & 2u) apply_u2<R, LR, 1, CTL>(a, D, gq, greg);
-  if constexpr (LR > 2) if (act & 4u) apply_u2<R, LR, 2, CTL>(a, D, gq, greg);
-  if constexpr (LR > 3) if (act & 8u) apply_u2<R, LR, 3, CTL>(a, D, gq, greg);
-  if constexpr (LR > 4) if (act & 16u) apply_u2<R, LR, 4, CTL>(a, D, gq, greg);
+  if (act & 1u) apply_u2<R, LR, 0, CTL, REAL>(a, D, gq, greg);
+  if constexpr (LR > 1) if (act & 2u) apply_u2<R, LR, 1, CTL, REAL>(a, D, gq, greg);
+  if constexpr (LR > 2) if (act & 4u) apply_u2<R, LR, 2, CTL, REAL>(a, D, gq, greg);
+  if constexpr (LR > 3) if (act & 8u) apply_u2<R, LR, 3, CTL, REAL>(a, D, gq, greg);
+  if constexpr (LR > 4) if (act & 16u) apply_u2<R, LR, 4, CTL, REAL>(a, D, gq, greg);
 }
 
 // One QFT stage on register bit K (forward: butterfly then phase; inverse:
@@ -368,17 +405,6 @@ __device__ __forceinline__ void apply_regdiag(V2<R> (&a)[16], const V2<R>* lut, 
   for (int r = 0; r < 16; ++r) a[r] = cmul(a[r], cmul(f, tr[r]));
 }
 
-template <int M>
-__device__ __forceinline__ uint32_t tile_base_of(uint32_t tile, const TileParams& P) {
-  uint64_t x = tile;
-#pragma unroll
-  for (int k = 0; k < M; ++k) {
-    const int pb = P.tile_bit[k];
-    x = ((x >> pb) << (pb + 1)) | (x & ((uint64_t(1) << pb) - 1));
-  }
-  return (uint32_t)x;
-}
-
 // Tile of 2^M amplitudes, 2^LT threads, 2^LR amplitudes per register
 // group.  Global traffic moves in 16-byte chunks (two complex64 or one
 // complex128 amplitude): chunk c covers tile-local element c << CB.
@@ -410,14 +436,15 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   constexpr int NCH = E >> CB;                         // chunks per tile
   constexpr int CPT = NCH / NT;                        // chunks per thread
   constexpr int LCH = (M - CB) - LT;                   // chunk-index bits above the thread bits
+  constexpr int NBUF = tile_nbuf(M, LT);
   static_assert(GPT >= 1 && CPT >= 1, "bad tile configuration");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* bufs = reinterpret_cast<T*>(smem_raw);
-  PhaseDesc* phs = reinterpret_cast<PhaseDesc*>(smem_raw + 2 * sizeof(T) * E);
+  PhaseDesc* phs = reinterpret_cast<PhaseDesc*>(smem_raw + NBUF * sizeof(T) * E);
   const float2* tw = nullptr;
   // MODE 2: permutation columns, then the diagonal tables
-  uint32_t* ecols = reinterpret_cast<uint32_t*>(smem_raw + 2 * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases);
-  T* elut = reinterpret_cast<T*>(smem_raw + 2 * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases + 128);
+  uint32_t* ecols = reinterpret_cast<uint32_t*>(smem_raw + NBUF * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases);
+  T* elut = reinterpret_cast<T*>(smem_raw + NBUF * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases + 128);
   const int tid = threadIdx.x;
   {
     const uint32_t words = (uint32_t)(sizeof(PhaseDesc) * P.n_phases / 4);
@@ -518,36 +545,40 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   auto src_base = [&](uint32_t t, uint32_t& cl) -> uint32_t {
     cl = 0;
     if constexpr (STORE_EPI) {
-      if (!P.epi.perm) return tile_base_of<M>(t, P);
+      if (!P.epi.perm) return deposit_runs(t, P.runs);
       const uint32_t b = P.epi.c ^ htab[t & 255u] ^ htab[256 + ((t >> 8) & 255u)] ^ htab[512 + ((t >> 16) & 255u)];
       cl = b & (uint32_t)(E - 1);
       return b & ~(uint32_t)(E - 1);
     } else {
-      return tile_base_of<M>(t, P);
+      return deposit_runs(t, P.runs);
     }
   };
   uint32_t tile = blockIdx.x;
-  if (tile < P.n_tiles) {
+  auto load_tile = [&](uint32_t t, T* buf) {
     uint32_t cl;
-    const uint32_t gb = src_base(tile, cl) | g_t;
-    const uint32_t sb = smem_u32(bufs);
+    const uint32_t gb = src_base(t, cl) | g_t;
+    const uint32_t sb = smem_u32(buf);
 #pragma unroll
     for (int k = 0; k < CPT; ++k) cp_async<16>(sb + 16u * slot(k), src + (gb | g_k(k)));
+  };
+  if constexpr (NBUF == 2) {
+    if (tile < P.n_tiles) load_tile(tile, bufs);
+    cp_async_commit();
   }
-  cp_async_commit();
   T a[NR];
   for (int it = 0; tile < P.n_tiles; tile += gridDim.x, ++it) {
-    T* cur = bufs + (it & 1) * E;
-    const uint32_t next = tile + gridDim.x;
-    if (next < P.n_tiles) {
-      uint32_t cl;
-      const uint32_t gb = src_base(next, cl) | g_t;
-      const uint32_t sb = smem_u32(bufs + ((it + 1) & 1) * E);
-#pragma unroll
-      for (int k = 0; k < CPT; ++k) cp_async<16>(sb + 16u * slot(k), src + (gb | g_k(k)));
+    T* cur = bufs + (NBUF == 2 ? (it & 1) * E : 0);
+    if constexpr (NBUF == 2) {
+      const uint32_t next = tile + gridDim.x;
+      if (next < P.n_tiles) load_tile(next, bufs + ((it + 1) & 1) * E);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      // the buffer is free: the previous tile's write-back ended with a barrier
+      load_tile(tile, bufs);
+      cp_async_commit();
+      cp_async_wait<0>();
     }
-    cp_async_commit();
-    cp_async_wait<1>();
     __syncthreads();
     uint32_t cl_in;
     const uint32_t base = src_base(tile, cl_in);
@@ -556,13 +587,23 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
       uint32_t greg[LR], sreg[LR];
 #pragma unroll
       for (int k = 0; k < LR; ++k) { greg[k] = D.g_reg[k]; sreg[k] = D.s_reg[k]; }
+      // the group's global index is read only by controlled gates, QFT
+      // twiddles and register-phase diagonals
+      bool need_g = QFT || D.any_ctl;
+      if constexpr (EPI && LR == 4)
+        need_g = need_g || (ph == 0 && P.epi.pre.on) || (ph == P.n_phases - 1 && P.epi.dreg);
 #pragma unroll
       for (int g = 0; g < GPT; ++g) {
         const uint32_t q = (uint32_t)tid + (uint32_t)g * NT;
         uint32_t sq = 0, gq = base;
 #pragma unroll
         for (int j = 0; j < M - LR; ++j)
-          if ((q >> j) & 1) { sq ^= D.s_grp[j]; gq |= D.g_grp[j]; }
+          if ((q >> j) & 1) sq ^= D.s_grp[j];
+        if (need_g) {
+#pragma unroll
+          for (int j = 0; j < M - LR; ++j)
+            if ((q >> j) & 1) gq |= D.g_grp[j];
+        }
         // complex64 with tile bit 0 in register slot 0: amplitudes r, r+1 share
         // one 16-byte chunk, read as one vector (a quarter-warp then covers
         // all eight chunk slots of a row)
@@ -589,8 +630,8 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
             apply_qft_op<R, LR>(a, P.ops[o], gq, treg, tw);
           }
         } else {
-          if (D.any_ctl) apply_u2_phase<R, LR, true>(a, D, gq, greg);
-          else apply_u2_phase<R, LR, false>(a, D, gq, greg);
+          if (D.any_ctl) apply_u2_phase<R, LR, true, (MODE < 2)>(a, D, gq, greg);
+          else apply_u2_phase<R, LR, false, (MODE < 2)>(a, D, gq, greg);
         }
         if constexpr (EPI && LR == 4) {
           if (P.epi.dreg && ph == P.n_phases - 1) {
@@ -659,7 +700,18 @@ struct Sweep {
   bool need_tw = false;
   double scale = 1.0;
   bool has_scale = false;
+  // rotation matrices may run in tangent form (PhaseDesc::rot); the caller
+  // multiplies the product of their factors (rot_factor) into a diagonal
+  bool rot = false;
 };
+
+static bool rot_enabled() {
+  const char* v = std::getenv("MQ_ROT");
+  return !(v && v[0] == '0');
+}
+// The factor a rotation row pair keeps out of its tangent form: c when
+// |c| >= |s| (then |t| <= 1), else s.
+static double rot_factor(double c, double s) { return std::fabs(c) >= std::fabs(s) ? c : s; }
 
 static int env_int(const char* name, int dflt, int lo, int hi) {
   const char* v = std::getenv(name);
@@ -684,6 +736,13 @@ static bool euler_enabled(const mq_state* h) {
   return h->n >= env_int("MQ_EULER_MIN_QUBITS", 20, 1, 32);
 }
 static int min_tile() { return env_int("MQ_TILE_MIN", 10, 1, 12); }
+// The Euler layer's sweeps fill their tiles to 12 bits with low passengers:
+// a 7-bit sweep then moves 256-byte runs (fused config layer at 30 qubits
+// 17.9 -> 16.3 ms); the complex sweeps measured slower that way.
+static int euler_min_tile() { return env_int("MQ_EULER_TILE_MIN", 12, 1, 12); }
+// Threads of a 13-bit complex64 tile: 2^9 with two tile buffers, or 2^8
+// with one (three CTAs per SM).
+static int tile13_lt() { return env_int("MQ_TILE13_LT", 9, 8, 9); }
 
 // Register phases: targets (tile-local) chunked in the given order into
 // groups of LR; the last group is padded with the highest tile bits it does
@@ -715,6 +774,8 @@ static void make_phases(int m, int lr, const std::vector<int>& order, Sweep& sw,
 template <typename R, int M, int LR, int LT, int MODE, typename PT>
 static int launch_tile_t(mq_state* h, const PT& P, size_t smem, bool out_of_place) {
   auto kern = k_tile<R, M, LR, LT, MODE, PT>;
+  // the caller sized shared memory for two tile buffers
+  if (tile_nbuf(M, LT) == 1) smem -= sizeof(V2<R>) << M;
   // the opt-in shared-memory limit only grows; resident CTAs per SM depend on
   // this launch's shared memory (rounded up to 1 KiB), looked up per size
   static std::mutex mu;
@@ -767,7 +828,10 @@ static int dispatch_tile_lr(mq_state* h, const PT& P, size_t smem, bool oop) {
       }
       break;
     case 13:
-      if constexpr (sizeof(R) == 4 && LR == 4) return launch_tile_t<R, 13, 4, 9, MODE, PT>(h, P, smem, oop);
+      if constexpr (sizeof(R) == 4 && LR == 4) {
+        if (tile13_lt() == 8) return launch_tile_t<R, 13, 4, 8, MODE, PT>(h, P, smem, oop);
+        return launch_tile_t<R, 13, 4, 9, MODE, PT>(h, P, smem, oop);
+      }
       break;
     default: break;
   }
@@ -918,10 +982,11 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
   P.n_phases = (uint8_t)sw.phases.size();
   P.n_ops = (uint8_t)sw.ops.size();
   for (int k = 0; k < m; ++k) P.tile_bit[k] = (uint8_t)sw.tile_bits[k];
+  make_base_runs(P.runs, h->n, P.tile_bit, m);
   // chunk-index bits above the thread bits: contiguous global bits?
   {
     const int cb = h->dtype == MQ_C64 ? 1 : 0;
-    const int lt = (m == 12 && lr == 5) ? 7 : (m == 13 ? 9 : std::min(8, m - lr));
+    const int lt = (m == 12 && lr == 5) ? 7 : (m == 13 ? tile13_lt() : std::min(8, m - lr));
     const int first = cb + lt;
     bool contig = true;
     for (int b = first + 1; b < m; ++b)
@@ -976,6 +1041,17 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
       for (int j = 0; j < 8; ++j) {
         D.ud[k][j] = sw.ops[o].u[j];
         D.uf[k][j] = (float)sw.ops[o].u[j];
+      }
+      const double* u = sw.ops[o].u;
+      if (sw.rot && !sw.mats_dev && ((D.real >> k) & 1u) && u[0] == u[6] && u[2] == -u[4] &&
+          (u[0] != 0.0 || u[4] != 0.0)) {
+        const double c = u[0], sn = u[4];
+        const bool b = rot_factor(c, sn) != c;
+        const double t = b ? c / sn : sn / c;
+        D.rot |= (uint8_t)(1u << k);
+        if (b) D.rotB |= (uint8_t)(1u << k);
+        D.ud[k][0] = t;
+        D.uf[k][0] = (float)t;
       }
     }
   }
@@ -1033,13 +1109,13 @@ static int tile_local(const std::vector<int>& bits, int gbit) {
 
 // Tile bits for a set of target bits: the targets, the low passengers, and
 // further low bits until the tile has at least min(n, MQ_TILE_MIN) bits.
-static std::vector<int> tile_for(int n, const std::vector<int>& targets, int pas, int tmax) {
+static std::vector<int> tile_for(int n, const std::vector<int>& targets, int pas, int tmax, int tmin) {
   std::vector<int> bits = targets;
   const int lowest = *std::min_element(targets.begin(), targets.end());
   for (int b = 0; b < std::min(std::max(pas, 1), lowest); ++b) bits.push_back(b);
   std::sort(bits.begin(), bits.end());
   bits.erase(std::unique(bits.begin(), bits.end()), bits.end());
-  const int want = std::min({n, min_tile(), tmax});
+  const int want = std::min({n, tmin, tmax});
   for (int b = 0; (int)bits.size() < want && b < n; ++b)
     if (std::find(bits.begin(), bits.end(), b) == bits.end()) bits.push_back(b);
   std::sort(bits.begin(), bits.end());
@@ -1053,8 +1129,13 @@ static std::vector<std::pair<int, int>> split_bits(int n, int tmax, int pas) {
   std::vector<std::pair<int, int>> groups;
   if (n <= tmax) { groups.push_back({0, n}); return groups; }
   const int hi_cap = tmax - pas;
-  const int n_hi = (n - tmax + hi_cap - 1) / hi_cap;
-  const int low = std::max(n - n_hi * hi_cap, std::min(tmax, (n + n_hi) / (n_hi + 1)));
+  int n_hi = (n - tmax + hi_cap - 1) / hi_cap;
+  int low = std::max(n - n_hi * hi_cap, std::min(tmax, (n + n_hi) / (n_hi + 1)));
+  const int want_low = env_int("MQ_SPLIT_LOW", 0, 0, tmax);
+  if (want_low > 0) {
+    low = want_low;
+    n_hi = (n - low + hi_cap - 1) / hi_cap;
+  }
   groups.push_back({0, low});
   int start = low;
   const int rest = n - low;
@@ -1069,7 +1150,8 @@ static std::vector<std::pair<int, int>> split_bits(int n, int tmax, int pas) {
 // The U(2) sweep of index bits [start, start+cnt): targets are the active
 // qubits among them.  Returns false when none is active.
 static bool build_u2_sweep(mq_state* h, const double* mats, const uint8_t* active, int start, int cnt, Sweep& sw,
-                           std::vector<int>& op_phase, std::vector<int>& op_rk, const double* mats_dev = nullptr) {
+                           std::vector<int>& op_phase, std::vector<int>& op_rk, const double* mats_dev = nullptr,
+                           int tmin = -1) {
   const int n = h->n;
   std::vector<int> gbits, qubits;
   for (int b = start + cnt - 1; b >= start; --b) {
@@ -1079,7 +1161,7 @@ static bool build_u2_sweep(mq_state* h, const double* mats, const uint8_t* activ
     qubits.push_back(q);
   }
   if (gbits.empty()) return false;
-  sw.tile_bits = tile_for(n, gbits, passengers(), tile_max(h->dtype));
+  sw.tile_bits = tile_for(n, gbits, passengers(), tile_max(h->dtype), tmin > 0 ? tmin : min_tile());
   const int m = (int)sw.tile_bits.size();
   const int lr = reg_bits(h->dtype, m);
   std::vector<int> order;
@@ -1167,9 +1249,18 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
   post_p.push_back(alpha_sum); post_p.insert(post_p.end(), 7, 0.0);
   const auto groups = split_bits(n, tile_max(h->dtype), passengers());
   const int max_entries = kEpiLutBytes / (int)h->amp_bytes();
+  // RY sweeps in tangent form: the product of the factors they leave out
+  // rides on the low sweep's register diagonal
+  const bool rot = rot_enabled();
+  double rot_scale = 1.0;
+  if (rot)
+    for (int q = 0; q < n; ++q) rot_scale *= rot_factor(ry[(size_t)q * 8], ry[(size_t)q * 8 + 4]);
   Sweep low;
   std::vector<int> low_phase, low_rk;
-  if (!build_u2_sweep(h, ry.data(), nullptr, groups[0].first, groups[0].second, low, low_phase, low_rk)) return MQ_OK;
+  const int tmin = euler_min_tile();
+  if (!build_u2_sweep(h, ry.data(), nullptr, groups[0].first, groups[0].second, low, low_phase, low_rk, nullptr, tmin))
+    return MQ_OK;
+  low.rot = rot;
   const int m = (int)low.tile_bits.size();
   if (low.phases.empty() || low.phases.back().size() != 4 || low.phases.front().size() != 4) return MQ_OK;
   EpiPlan e;
@@ -1185,6 +1276,8 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
     }
     if (e.reg.win.n < 0) return MQ_OK;
     e.dreg = true;
+    // every amplitude takes exactly one entry of T (entries [t_off, end))
+    for (size_t j = 2 * (size_t)e.reg.t_off; j < e.reg.win.vals.size(); ++j) e.reg.win.vals[j] *= rot_scale;
   }
   // the first sweep executed carries the pre diagonal
   Sweep first;
@@ -1192,7 +1285,8 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
   EpiPlan e_first;
   const bool has_high = groups.size() > 1 &&
                         build_u2_sweep(h, ry.data(), nullptr, groups[1].first, groups[1].second, first, first_phase,
-                                       first_rk);
+                                       first_rk, nullptr, tmin);
+  first.rot = rot;
   {
     const Sweep& fs = has_high ? first : low;
     if (fs.phases.empty() || fs.phases.front().size() != 4) return MQ_OK;
@@ -1227,7 +1321,9 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
     } else {
       Sweep sw;
       std::vector<int> op_phase, op_rk;
-      if (!build_u2_sweep(h, ry.data(), nullptr, groups[g].first, groups[g].second, sw, op_phase, op_rk)) continue;
+      if (!build_u2_sweep(h, ry.data(), nullptr, groups[g].first, groups[g].second, sw, op_phase, op_rk, nullptr, tmin))
+        continue;
+      sw.rot = rot;
       rc = run_sweep(h, sw, op_phase, op_rk);
     }
     if (rc) return rc;
@@ -1267,7 +1363,7 @@ int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_t
   std::vector<int> low_phase, low_rk;
   const bool low_u2 = u2 && build_u2_sweep(h, mats, active, groups[0].first, groups[0].second, low, low_phase, low_rk,
                                            mats_dev);
-  if (!low_u2) low.tile_bits = tile_for(n, {0}, passengers(), tile_max(h->dtype));
+  if (!low_u2) low.tile_bits = tile_for(n, {0}, passengers(), tile_max(h->dtype), min_tile());
   const int m = (int)low.tile_bits.size();
   EpiPlan e;
   if (n_terms > 0) {
@@ -1366,7 +1462,7 @@ int launch_qft_stages(mq_state* h, int q0, int k, int j_begin, int j_end, int in
     std::vector<int> gbits;
     for (int j : stages) gbits.push_back(n - 1 - q0 - j);
     Sweep sw;
-    sw.tile_bits = tile_for(n, gbits, pas, tmax);
+    sw.tile_bits = tile_for(n, gbits, pas, tmax, min_tile());
     const int m = (int)sw.tile_bits.size();
     if (m > tmax) return fail(MQ_EINVAL, "qft tile too large");
     const int lr = reg_bits(h->dtype, m);
@@ -1419,7 +1515,7 @@ int launch_cu2_list(mq_state* h, int n_gates, const int32_t* targets, const uint
     std::vector<int> gbits;
     for (int i : members) gbits.push_back(n - 1 - targets[i]);
     Sweep sw;
-    sw.tile_bits = tile_for(n, gbits, pas, tmax);
+    sw.tile_bits = tile_for(n, gbits, pas, tmax, min_tile());
     const int m = (int)sw.tile_bits.size();
     if (m > tmax) return fail(MQ_EINVAL, "controlled-gate tile too large");
     const int lr = reg_bits(h->dtype, m);

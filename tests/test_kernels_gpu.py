@@ -385,6 +385,37 @@ def test_euler_split_layer_equals_complex_sweeps(dtype, monkeypatch):
         assert _err(out[flag], ref.state) <= TOL[dtype], flag
 
 
+@pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
+@pytest.mark.parametrize("n", [4, 9, 12, 13, 17, 21])
+def test_euler_tangent_rotations(n, dtype, monkeypatch):
+    """The Euler split's RY gates in tangent form (one FMA per output
+    component, the cos / sin factors multiplied into the low sweep's
+    diagonal) equal the oracle's gate-by-gate layer, with the edge angles
+    that select each form: identity, X and Z (c or s exactly 0), Hadamard,
+    RY(pi/2) (|c| = |s|), and Haar U(2)s on the other qubits."""
+    from mettleq_b200 import fusion as F
+    monkeypatch.setenv("MQ_EULER_MIN_QUBITS", "1")
+    rng = np.random.default_rng(500 + n)
+    special = [np.eye(2), np.array([[0, 1], [1, 0]]), np.diag([1, -1]),
+               np.array([[1, 1], [1, -1]]) / math.sqrt(2.0),
+               np.array([[1, -1], [1, 1]]) / math.sqrt(2.0)]
+    mats = np.stack([(special[q].astype(np.complex128) if q < len(special) else haar_u2(rng)).reshape(4)
+                     for q in range(n)])
+    terms = [(F.DIAG_ZZ, i, i + 1, [float(rng.uniform(0, math.pi))]) for i in range(n - 1)]
+    rows, c = _ladder(n)
+    vec = rand_state(n, 11 + n, dtype)
+    for flag in ("1", "0"):
+        monkeypatch.setenv("MQ_ROT", flag)
+        sv = _sv(n, dtype, vec)
+        sv.apply_layer(mats, None, terms, rows, c)
+        sv.apply_layer(mats[::-1].copy(), None, terms, rows, c)
+        got = sv.get()
+        sv.close()
+        ref = _layer_reference(n, vec, mats, None, terms, rows, c)
+        ref = _layer_reference(n, ref.astype(np.complex128), mats[::-1].copy(), None, terms, rows, c)
+        assert _err(got, ref) <= 2 * TOL[dtype], flag
+
+
 @pytest.mark.gpu
 def test_device_shots_agree_with_reference_probabilities():
     """1000 device shots from the reference's own 8-qubit state, against the
