@@ -136,6 +136,9 @@ struct EpiDesc {
   uint32_t n_entries;  // table entries (complex values of the state's type)
   uint32_t c;          // permutation flip constant
   uint32_t cols[32];   // permutation columns A e_j
+  // A (t << M) for tile index t = XOR of htab[256 k + byte k of t], k < 3
+  // (A is linear); read at a CTA-uniform index from the parameter space
+  uint32_t htab[768];
   alignas(16) unsigned char lut[kEpiLutBytes];
 };
 struct FusedParams : TileParams {
@@ -405,6 +408,9 @@ __device__ __forceinline__ void apply_regdiag(V2<R> (&a)[16], const V2<R>* lut, 
   for (int r = 0; r < 16; ++r) a[r] = cmul(a[r], cmul(f, tr[r]));
 }
 
+#ifndef MQ_MODE2_CTAS
+#define MQ_MODE2_CTAS 3
+#endif
 // Tile of 2^M amplitudes, 2^LT threads, 2^LR amplitudes per register
 // group.  Global traffic moves in 16-byte chunks (two complex64 or one
 // complex128 amplitude): chunk c covers tile-local element c << CB.
@@ -422,7 +428,7 @@ __device__ __forceinline__ void apply_regdiag(V2<R> (&a)[16], const V2<R>* lut, 
 // window-diagonal write-back needs the tile bits [0, M)); MODE 3: U(2) phases
 // with register-phase diagonals only and the plain write-back.
 template <typename R, int M, int LR, int LT, int MODE, typename PT>
-__global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? (MODE == 2 ? 2 : 3) : (LT >= 7 ? (sizeof(R) == 4 && LR == 4 ? 6 : 3) : (LT >= 6 && sizeof(R) == 4 ? 8 : 1)))))
+__global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? (MODE == 2 ? MQ_MODE2_CTAS : 3) : (LT >= 7 ? (sizeof(R) == 4 && LR == 4 ? 6 : 3) : (LT >= 6 && sizeof(R) == 4 ? 8 : 1)))))
 k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   using T = V2<R>;
   constexpr bool QFT = MODE == 1;
@@ -443,8 +449,11 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   PhaseDesc* phs = reinterpret_cast<PhaseDesc*>(smem_raw + NBUF * sizeof(T) * E);
   const float2* tw = nullptr;
   // MODE 2: permutation columns, then the diagonal tables
-  uint32_t* ecols = reinterpret_cast<uint32_t*>(smem_raw + NBUF * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases);
-  T* elut = reinterpret_cast<T*>(smem_raw + NBUF * sizeof(T) * E + sizeof(PhaseDesc) * kMaxPhases + 128);
+  // shared memory: tile buffers, the launch's phase descriptors, then (MODE
+  // >= 2) the permutation columns and the diagonal tables
+  const size_t ph_end = NBUF * sizeof(T) * E + sizeof(PhaseDesc) * P.n_phases;
+  uint32_t* ecols = reinterpret_cast<uint32_t*>(smem_raw + ph_end);
+  T* elut = reinterpret_cast<T*>(smem_raw + ph_end + 128);
   const int tid = threadIdx.x;
   {
     const uint32_t words = (uint32_t)(sizeof(PhaseDesc) * P.n_phases / 4);
@@ -476,24 +485,6 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   __syncthreads();
 
   if constexpr (QFT) tw = g_qft_twiddles;
-  // MODE 2 with a permutation: A (t << M) for tile index t as three 8-bit
-  // lookup tables (A is linear: the XOR of the columns of t's set bits)
-  uint32_t* htab = reinterpret_cast<uint32_t*>(elut);
-  if constexpr (STORE_EPI) {
-    htab = reinterpret_cast<uint32_t*>(elut + ((P.epi.n_entries + 1u) & ~1u));
-    if (P.epi.perm) {
-      for (int e = tid; e < 768; e += NT) {
-        const int k = e >> 8, x = e & 255;
-        uint32_t v = 0;
-        for (int bit = 0; bit < 8; ++bit) {
-          const int j = M + 8 * k + bit;
-          if (((x >> bit) & 1) && j < (int)P.n) v ^= ecols[j];
-        }
-        htab[e] = v;
-      }
-      __syncthreads();
-    }
-  }
   // MODE 2 with a permutation: A applied to the low offsets of this thread's
   // output chunks (c = tid + k*NT -> amplitude c << CB), computed once
   uint32_t epi_ak[STORE_EPI ? CPT : 1];
@@ -546,7 +537,8 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
     cl = 0;
     if constexpr (STORE_EPI) {
       if (!P.epi.perm) return deposit_runs(t, P.runs);
-      const uint32_t b = P.epi.c ^ htab[t & 255u] ^ htab[256 + ((t >> 8) & 255u)] ^ htab[512 + ((t >> 16) & 255u)];
+      const uint32_t b =
+          P.epi.c ^ P.epi.htab[t & 255u] ^ P.epi.htab[256 + ((t >> 8) & 255u)] ^ P.epi.htab[512 + ((t >> 16) & 255u)];
       cl = b & (uint32_t)(E - 1);
       return b & ~(uint32_t)(E - 1);
     } else {
@@ -909,6 +901,14 @@ static void fill_epi(EpiDesc& D, const EpiPlan& e, int m, int n) {
   if (e.perm) {
     for (int j = 0; j < n; ++j) D.cols[j] = e.cols[j];
     D.c = e.c;
+    for (int x = 0; x < 768; ++x) {
+      uint32_t v = 0;
+      for (int bit = 0; bit < 8; ++bit) {
+        const int j = m + 8 * (x >> 8) + bit;
+        if (((x >> bit) & 1) && j < n) v ^= e.cols[j];
+      }
+      D.htab[x] = v;
+    }
   }
   uint32_t used = 0;
   if (e.pre) {
@@ -1059,7 +1059,7 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
   P.need_tw = (qft && sw.need_tw && h->dtype == MQ_C64) ? 1 : 0;
   P.has_scale = sw.has_scale ? 1 : 0;
   P.scale = sw.has_scale ? sw.scale : 1.0;
-  size_t smem = 2 * (h->amp_bytes() << m) + sizeof(PhaseDesc) * kMaxPhases;
+  size_t smem = 2 * (h->amp_bytes() << m) + sizeof(PhaseDesc) * sw.phases.size();
   if (P.need_tw) {
     int rc = ensure_qft_twiddles(h);
     if (rc) return rc;
@@ -1068,7 +1068,7 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
     if (qft) return fail(MQ_EINVAL, "fused epilogue on a QFT sweep");
     if (h->dtype == MQ_C64) fill_epi<float>(F.epi, *epi, m, h->n);
     else fill_epi<double>(F.epi, *epi, m, h->n);
-    smem += 128 + (size_t)((F.epi.n_entries + 1u) & ~1u) * h->amp_bytes() + (F.epi.perm ? 768 * 4 : 0);
+    smem += 128 + (size_t)((F.epi.n_entries + 1u) & ~1u) * h->amp_bytes();
     if (epi->perm || epi->diag) {
       if (h->dtype == MQ_C64) return dispatch_tile<float, 2>(h, F, smem, epi->perm);
       return dispatch_tile<double, 2>(h, F, smem, epi->perm);
