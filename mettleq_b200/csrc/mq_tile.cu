@@ -734,7 +734,11 @@ static int min_tile() { return env_int("MQ_TILE_MIN", 10, 1, 12); }
 static int euler_min_tile() { return env_int("MQ_EULER_TILE_MIN", 12, 1, 12); }
 // Threads of a 13-bit complex64 tile: 2^9 with two tile buffers, or 2^8
 // with one (three CTAs per SM).
-static int tile13_lt() { return env_int("MQ_TILE13_LT", 9, 8, 9); }
+static int tile13_lt() { return env_int("MQ_TILE13_LT", 8, 8, 9); }
+// Euler layers: a high sweep of 8 target bits as a 13-bit tile with five
+// passengers (256-byte runs, one tile buffer) instead of a 12-bit one
+// (fused config layer at 27 qubits 1.94 -> 1.87 ms, at 30 qubits 15.6 -> 15.5 ms).
+static bool euler_hi13() { return env_int("MQ_EULER_HI13", 1, 0, 1) == 1; }
 
 // Register phases: targets (tile-local) chunked in the given order into
 // groups of LR; the last group is padded with the highest tile bits it does
@@ -743,13 +747,20 @@ static int tile13_lt() { return env_int("MQ_TILE13_LT", 9, 8, 9); }
 // free of bank conflicts.  Records the phase index and register slot of
 // every target.
 static void make_phases(int m, int lr, const std::vector<int>& order, Sweep& sw, std::vector<int>& op_phase,
-                        std::vector<int>& op_rk) {
+                        std::vector<int>& op_rk, bool pad_first = false) {
   sw.phases.clear();
   op_phase.assign(order.size(), 0);
   op_rk.assign(order.size(), 0);
-  for (size_t i = 0; i < order.size(); i += lr) {
+  // pad_first: the first group takes the remainder, so that targets given
+  // from the highest bit down fill the lower groups whole (a low sweep's
+  // groups then sit on 4-bit boundaries, where register phases are free of
+  // bank conflicts)
+  const size_t rem = order.size() % (size_t)lr;
+  const size_t first = (pad_first && rem) ? rem : (size_t)lr;
+  for (size_t i = 0; i < order.size(); i += (i == 0 ? first : (size_t)lr)) {
+    const size_t cnt = i == 0 ? first : (size_t)lr;
     std::vector<int> regs;
-    for (size_t j = i; j < std::min(order.size(), i + lr); ++j) {
+    for (size_t j = i; j < std::min(order.size(), i + cnt); ++j) {
       op_phase[j] = (int)sw.phases.size();
       regs.push_back(order[j]);
     }
@@ -757,7 +768,7 @@ static void make_phases(int m, int lr, const std::vector<int>& order, Sweep& sw,
       if (std::find(regs.begin(), regs.end(), b) == regs.end()) regs.push_back(b);
     std::vector<int> sorted = regs;
     std::sort(sorted.begin(), sorted.end());
-    for (size_t j = i; j < std::min(order.size(), i + lr); ++j)
+    for (size_t j = i; j < std::min(order.size(), i + cnt); ++j)
       op_rk[j] = (int)(std::find(sorted.begin(), sorted.end(), order[j]) - sorted.begin());
     sw.phases.push_back(sorted);
   }
@@ -966,7 +977,8 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
                      const EpiPlan* epi = nullptr) {
   const int m = (int)sw.tile_bits.size();
   const int lr = epi ? std::min(m, 4) : reg_bits(h->dtype, m);
-  if (m < 1 || m > tile_max(h->dtype) || m > h->n) return fail(MQ_EINVAL, "bad tile size");
+  if (m < 1 || m > std::max(tile_max(h->dtype), h->dtype == MQ_C64 && lr == 4 ? kTileMaxC64 : 0) || m > h->n)
+    return fail(MQ_EINVAL, "bad tile size");
   if (sw.tile_bits[0] != 0) return fail(MQ_EINVAL, "tile must contain index bit 0");
   if ((int)sw.ops.size() > kMaxOps || (int)sw.phases.size() > kMaxPhases) return fail(MQ_EINVAL, "tile plan too large");
   if (epi && (epi->perm || epi->diag))
@@ -1161,12 +1173,15 @@ static bool build_u2_sweep(mq_state* h, const double* mats, const uint8_t* activ
     qubits.push_back(q);
   }
   if (gbits.empty()) return false;
-  sw.tile_bits = tile_for(n, gbits, passengers(), tile_max(h->dtype), tmin > 0 ? tmin : min_tile());
+  // a caller's minimum above the planner's maximum (13-bit complex64 tiles)
+  // raises the maximum with it
+  const int tmax = (h->dtype == MQ_C64 && tmin > tile_max(h->dtype)) ? std::min(tmin, kTileMaxC64) : tile_max(h->dtype);
+  sw.tile_bits = tile_for(n, gbits, passengers(), tmax, tmin > 0 ? tmin : min_tile());
   const int m = (int)sw.tile_bits.size();
   const int lr = reg_bits(h->dtype, m);
   std::vector<int> order;
   for (int b : gbits) order.push_back(tile_local(sw.tile_bits, b));
-  make_phases(m, lr, order, sw, op_phase, op_rk);
+  make_phases(m, lr, order, sw, op_phase, op_rk, env_int("MQ_PAD_FIRST", 1, 0, 1) == 1);
   for (size_t i = 0; i < order.size(); ++i) {
     TileOp op;
     std::memset(&op, 0, sizeof(op));
@@ -1258,6 +1273,8 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
   Sweep low;
   std::vector<int> low_phase, low_rk;
   const int tmin = euler_min_tile();
+  const bool hi13 = h->dtype == MQ_C64 && euler_hi13() && reg_bits(MQ_C64, 13) == 4;
+  auto hi_tmin = [&](int cnt) { return (hi13 && cnt + 5 > tmin) ? kTileMaxC64 : tmin; };
   if (!build_u2_sweep(h, ry.data(), nullptr, groups[0].first, groups[0].second, low, low_phase, low_rk, nullptr, tmin))
     return MQ_OK;
   low.rot = rot;
@@ -1285,7 +1302,7 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
   EpiPlan e_first;
   const bool has_high = groups.size() > 1 &&
                         build_u2_sweep(h, ry.data(), nullptr, groups[1].first, groups[1].second, first, first_phase,
-                                       first_rk, nullptr, tmin);
+                                       first_rk, nullptr, hi_tmin(groups[1].second));
   first.rot = rot;
   {
     const Sweep& fs = has_high ? first : low;
@@ -1321,7 +1338,8 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
     } else {
       Sweep sw;
       std::vector<int> op_phase, op_rk;
-      if (!build_u2_sweep(h, ry.data(), nullptr, groups[g].first, groups[g].second, sw, op_phase, op_rk, nullptr, tmin))
+      if (!build_u2_sweep(h, ry.data(), nullptr, groups[g].first, groups[g].second, sw, op_phase, op_rk, nullptr,
+                          hi_tmin(groups[g].second)))
         continue;
       sw.rot = rot;
       rc = run_sweep(h, sw, op_phase, op_rk);

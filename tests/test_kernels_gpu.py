@@ -385,8 +385,8 @@ def test_euler_split_layer_equals_complex_sweeps(dtype, monkeypatch):
         assert _err(out[flag], ref.state) <= TOL[dtype], flag
 
 
-@pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
-@pytest.mark.parametrize("n", [4, 9, 12, 13, 17, 21])
+@pytest.mark.parametrize("dtype,n", [(d, n) for d in (np.complex64, np.complex128) for n in (4, 9, 12, 13, 17, 21)]
+                         + [(np.complex64, 24)])
 def test_euler_tangent_rotations(n, dtype, monkeypatch):
     """The Euler split's RY gates in tangent form (one FMA per output
     component, the cos / sin factors multiplied into the low sweep's
@@ -404,6 +404,8 @@ def test_euler_tangent_rotations(n, dtype, monkeypatch):
     terms = [(F.DIAG_ZZ, i, i + 1, [float(rng.uniform(0, math.pi))]) for i in range(n - 1)]
     rows, c = _ladder(n)
     vec = rand_state(n, 11 + n, dtype)
+    ref = _layer_reference(n, vec, mats, None, terms, rows, c)
+    ref = _layer_reference(n, ref, mats[::-1].copy(), None, terms, rows, c)
     for flag in ("1", "0"):
         monkeypatch.setenv("MQ_ROT", flag)
         sv = _sv(n, dtype, vec)
@@ -411,8 +413,6 @@ def test_euler_tangent_rotations(n, dtype, monkeypatch):
         sv.apply_layer(mats[::-1].copy(), None, terms, rows, c)
         got = sv.get()
         sv.close()
-        ref = _layer_reference(n, vec, mats, None, terms, rows, c)
-        ref = _layer_reference(n, ref.astype(np.complex128), mats[::-1].copy(), None, terms, rows, c)
         assert _err(got, ref) <= 2 * TOL[dtype], flag
 
 
