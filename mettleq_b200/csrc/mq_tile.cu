@@ -1361,6 +1361,13 @@ int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_t
     uint32_t inv[32];
     if (!gf2_invert(n, cols, inv)) return fail(MQ_EINVAL, "affine map is not invertible over GF(2)");
   }
+  // a mask with every qubit set is the whole layer (the gate-stream fusion
+  // lists the active qubits even when all of them are)
+  if (active) {
+    bool all = true;
+    for (int q = 0; q < n; ++q) all = all && active[q];
+    if (all) active = nullptr;
+  }
   // the split pays when the layer carries a diagonal of its own, which the
   // RZ(phi) factors join at no extra cost; alone, its two diagonals cost more
   // than the real sweeps save

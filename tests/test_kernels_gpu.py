@@ -416,6 +416,27 @@ def test_euler_tangent_rotations(n, dtype, monkeypatch):
         assert _err(got, ref) <= 2 * TOL[dtype], flag
 
 
+def test_fused_layer_full_active_list_takes_the_whole_layer_path():
+    """The gate-stream fusion passes the list of active qubits even when it
+    holds every qubit; such a layer runs exactly as one with no list (the
+    Euler split included, from 20 qubits): bit-identical states."""
+    from mettleq_b200 import fusion as F
+    n = 21
+    rng = np.random.default_rng(91)
+    mats = np.stack([haar_u2(rng).reshape(4) for _ in range(n)])
+    terms = [(F.DIAG_ZZ, i, i + 1, [float(rng.uniform(0, math.pi))]) for i in range(n - 1)]
+    rows, c = _ladder(n)
+    vec = rand_state(n, 5)
+    out = []
+    for active in (None, list(range(n))):
+        sv = _sv(n, np.complex64, vec)
+        sv.apply_layer(mats, active, terms, rows, c)
+        out.append(sv.get())
+        sv.close()
+    assert np.array_equal(out[0], out[1])
+    assert _err(out[1], _layer_reference(n, vec, mats, None, terms, rows, c)) <= 1e-5
+
+
 @pytest.mark.gpu
 def test_device_shots_agree_with_reference_probabilities():
     """1000 device shots from the reference's own 8-qubit state, against the
