@@ -126,33 +126,68 @@ def measured_peaks():
 
 
 # ---------------------------------------------------------------- CPU side
-def cpu_baseline_sample(n_target: int, n_cpu: int, circuit, repeats: int = 1):
+def cpu_threads() -> int:
+    """Host threads the CPU baseline may use: the process's CPU affinity."""
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except Exception:
+        return max(1, os.cpu_count() or 1)
+
+
+def cpu_baseline_sample(n_target: int, n_cpu: int, circuit, repeats: int = 1, threads: int = 1):
     """Time the oracle (the reference's per-gate CPU algorithm restated in
     numpy) on a bounded sample: one U3-type gate, one ZZPHASE, one CNOT and
     one QFT ladder diagonal at n_cpu qubits; per-gate time scales with the
     state size (2^n), so times are scaled by 2^(n_target - n_cpu) and the
-    full circuit's per-gate schedule is extrapolated from them."""
+    full circuit's per-gate schedule is extrapolated from them.
+
+    With threads > 1 the n_cpu-qubit state is split along its top k qubits
+    into 2^k <= threads independent chunks, one per thread (numpy releases the
+    GIL inside its array loops): a gate on qubit q >= k is the same gate on
+    qubit q - k of every chunk, so the timed work is the full state's.  The
+    ladder diagonal is timed on each chunk's own qubits.  Returns (seconds,
+    sample description, threads used)."""
+    from concurrent.futures import ThreadPoolExecutor
     from oracle import OracleSim
-    rng = np.random.default_rng(1)
-    sim = OracleSim(n_cpu, np.complex64)
-    v = (rng.standard_normal(1 << n_cpu) + 1j * rng.standard_normal(1 << n_cpu)).astype(np.complex64)
-    sim.set_state(v / np.linalg.norm(v))
-    del v
-    mat = circuit.layers[0].mats[0].reshape(2, 2)
     q = n_cpu // 2
+    k = 0
+    while (2 << k) <= max(1, threads) and k + 1 < q:
+        k += 1
+    T = 1 << k
+    nl = n_cpu - k
+    rng = np.random.default_rng(1)
+    sims = []
+    for _ in range(T):
+        sim = OracleSim(nl, np.complex64)
+        v = (rng.standard_normal(1 << nl) + 1j * rng.standard_normal(1 << nl)).astype(np.complex64)
+        sim.set_state(v / np.linalg.norm(v))
+        sims.append(sim)
+        del v
+    mat = circuit.layers[0].mats[0].reshape(2, 2)
+    ql = q - k
+    pool = ThreadPoolExecutor(T) if T > 1 else None
+
+    def par(fn):
+        if pool is None:
+            fn(sims[0])
+        else:
+            list(pool.map(fn, sims))
 
     def t(fn):
         best = float("inf")
         for _ in range(repeats):
             t0 = time.perf_counter()
-            fn()
+            par(fn)
             best = min(best, time.perf_counter() - t0)
         return best
 
-    t_u = t(lambda: sim.apply_single(mat, q))
-    t_zz = t(lambda: sim.apply_zz_phase(0.3, q, q + 1))
-    t_cx = t(lambda: sim.apply_controlled_single(np.array([[0, 1], [1, 0]]), q, q + 1))
-    t_ld = t(lambda: sim._phase_ladder(list(range(n_cpu)), 0, 1.0))
+    cx = np.array([[0, 1], [1, 0]])
+    t_u = t(lambda s: s.apply_single(mat, ql))
+    t_zz = t(lambda s: s.apply_zz_phase(0.3, ql, ql + 1))
+    t_cx = t(lambda s: s.apply_controlled_single(cx, ql, ql + 1))
+    t_ld = t(lambda s: s._phase_ladder(list(range(nl)), 0, 1.0))
+    if pool is not None:
+        pool.shutdown()
     scale = 2.0 ** (n_target - n_cpu)
     t_u, t_zz, t_cx, t_ld = (x * scale for x in (t_u, t_zz, t_cx, t_ld))
     n = n_target
@@ -163,9 +198,10 @@ def cpu_baseline_sample(n_target: int, n_cpu: int, circuit, repeats: int = 1):
             total += n * (t_u + t_ld)
         if L.xor is not None:
             total += 2 * n * t_cx  # Gauss-Jordan synthesis is ~n^2/2 gates; count 2n as a lower bound
-    sample = (f"oracle per-gate numpy path at n={n_cpu}: 1 U(2), 1 ZZPHASE, 1 CNOT, 1 QFT ladder diagonal; "
+    split = f", split into {T} chunks of {nl} qubits on {T} threads" if T > 1 else ", one thread"
+    sample = (f"oracle per-gate numpy path at n={n_cpu}{split}: 1 U(2), 1 ZZPHASE, 1 CNOT, 1 QFT ladder diagonal; "
               f"times x2^{n_target - n_cpu} to n={n_target} and extrapolated over the circuit's gate schedule")
-    return total, sample
+    return total, sample, T
 
 
 # ---------------------------------------------------------------- our arm
@@ -338,8 +374,8 @@ def run_ours(args, rank, world, local_rank, dist):
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         n_cpu = min(args.cpu_qubits, n)
-        t_cpu, sample = cpu_baseline_sample(n, n_cpu, circuit)
-        out["cpu_baseline"] = {"value": logical * layer_bytes / t_cpu / 1e9, "unit": "GB/s", "cores": 1,
+        t_cpu, sample, used = cpu_baseline_sample(n, n_cpu, circuit, threads=cpu_threads())
+        out["cpu_baseline"] = {"value": logical * layer_bytes / t_cpu / 1e9, "unit": "GB/s", "cores": used,
                                "kind": "port", "sample": sample, "extrapolated_circuit_s": t_cpu}
     return out
 
@@ -522,10 +558,12 @@ def run_reference(args):
     logical = circuit.logical_layers()
     layer_bytes = 2 * (1 << n) * 8
     n_cpu = min(args.cpu_qubits, n)
-    cpu_baseline_sample(n, min(n_cpu, 20), circuit)  # warm the allocator / code paths
+    threads = cpu_threads()
+    cpu_baseline_sample(n, min(n_cpu, 20), circuit, threads=threads)  # warm the allocator / code paths
     times = []
+    used = 1
     for _ in range(max(1, args.steps)):
-        t_cpu, sample = cpu_baseline_sample(n, n_cpu, circuit)
+        t_cpu, sample, used = cpu_baseline_sample(n, n_cpu, circuit, threads=threads)
         times.append(t_cpu)
     t = statistics.median(times)
     value = logical * layer_bytes / t / 1e9
@@ -534,7 +572,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64", "data": "synthetic",
         "config": {"workload": f"scale: {n} qubits complex64, {args.layers} layers", "qubits": n},
-        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": 1, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": used, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "ms_per_step": t * 1e3,
     }
