@@ -57,24 +57,31 @@ def _is(m: np.ndarray, ref: np.ndarray) -> bool:
 def normalize(ops: Sequence[dict], n: int) -> List[dict]:
     """Canonical names, validated arity/wires/parameter counts."""
     out = []
+    append = out.append
+    names: Dict[Any, str] = {}  # raw name -> canonical name, per call
     for op in ops:
-        name = G.canonical_name(op.get("name", ""))
-        wires = [int(w) for w in op.get("wires", [])]
-        params = [float(p) for p in (op.get("parameters", []) or [])]
-        if name.startswith("_"):
-            out.append(dict(op))
+        raw = op.get("name", "")
+        name = names.get(raw)
+        if name is None:
+            name = names[raw] = G.canonical_name(raw)
+        wires = [int(w) for w in op.get("wires", ())]
+        params = [float(p) for p in (op.get("parameters") or ())]
+        if name[:1] == "_":
+            append(dict(op))
             continue
-        if name not in ARITIES:
-            raise ValueError(f"Unsupported operation: {op.get('name')}")
-        if len(wires) != ARITIES[name]:
-            raise ValueError(f"{name} expects {ARITIES[name]} wire(s), got {len(wires)}")
+        arity = ARITIES.get(name)
+        if arity is None:
+            raise ValueError(f"Unsupported operation: {raw}")
+        if len(wires) != arity:
+            raise ValueError(f"{name} expects {arity} wire(s), got {len(wires)}")
         if len(params) < PARAMS.get(name, 0):
             raise ValueError(f"{name} expects {PARAMS.get(name, 0)} parameter(s), got {len(params)}")
-        if any(not (0 <= w < n) for w in wires):
-            raise ValueError("Qubit index out of range")
-        if len(set(wires)) != len(wires):
+        for w in wires:
+            if not (0 <= w < n):
+                raise ValueError("Qubit index out of range")
+        if arity > 1 and len(set(wires)) != arity:
             raise ValueError("Control/target wires must be distinct")
-        out.append({"name": name, "wires": wires, "parameters": params})
+        append({"name": name, "wires": wires, "parameters": params})
     return out
 
 

@@ -75,10 +75,20 @@ def single_qubit_matrix(name: str, params: Sequence[float] = ()) -> np.ndarray:
     if name == "U1":
         return phase(p[0])
     if name == "U2":
-        return rz(p[0]) @ ry(math.pi / 2.0) @ rz(p[1])
+        return _u3(math.pi / 2.0, p[0], p[1])
     if name == "U3":
-        return rz(p[1]) @ ry(p[0]) @ rz(p[2])
+        return _u3(p[0], p[1], p[2])
     raise ValueError(f"Unsupported single-qubit op: {name}")
+
+
+def _u3(theta: float, phi: float, lam: float) -> np.ndarray:
+    """RZ(phi) RY(theta) RZ(lam) multiplied out:
+    [[e^{-i(phi+lam)/2} c, -e^{-i(phi-lam)/2} s], [e^{i(phi-lam)/2} s, e^{i(phi+lam)/2} c]]."""
+    c, s = math.cos(theta / 2.0), math.sin(theta / 2.0)
+    a, b = (phi + lam) / 2.0, (phi - lam) / 2.0
+    ca, sa, cb, sb = math.cos(a), math.sin(a), math.cos(b), math.sin(b)
+    return np.array([[complex(ca * c, -sa * c), complex(-cb * s, sb * s)],
+                     [complex(cb * s, sb * s), complex(ca * c, sa * c)]], dtype=np.complex128)
 
 
 def controlled_target_matrix(name: str, params: Sequence[float] = ()) -> np.ndarray:
