@@ -732,6 +732,8 @@ static int min_tile() { return env_int("MQ_TILE_MIN", 10, 1, 12); }
 // a 7-bit sweep then moves 256-byte runs (fused config layer at 30 qubits
 // 17.9 -> 16.3 ms); the complex sweeps measured slower that way.
 static int euler_min_tile() { return env_int("MQ_EULER_TILE_MIN", 12, 1, 12); }
+// ... and the low sweep's tile (its bits are contiguous: any size moves long runs)
+static int euler_low_tile() { return env_int("MQ_EULER_LOW_TILE", 12, 1, 12); }
 // Threads of a 13-bit complex64 tile: 2^9 with two tile buffers, or 2^8
 // with one (three CTAs per SM).
 static int tile13_lt() { return env_int("MQ_TILE13_LT", 8, 8, 9); }
@@ -1275,7 +1277,8 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
   const int tmin = euler_min_tile();
   const bool hi13 = h->dtype == MQ_C64 && euler_hi13() && reg_bits(MQ_C64, 13) == 4;
   auto hi_tmin = [&](int cnt) { return (hi13 && cnt + 5 > tmin) ? kTileMaxC64 : tmin; };
-  if (!build_u2_sweep(h, ry.data(), nullptr, groups[0].first, groups[0].second, low, low_phase, low_rk, nullptr, tmin))
+  if (!build_u2_sweep(h, ry.data(), nullptr, groups[0].first, groups[0].second, low, low_phase, low_rk, nullptr,
+                      euler_low_tile()))
     return MQ_OK;
   low.rot = rot;
   const int m = (int)low.tile_bits.size();
