@@ -741,6 +741,9 @@ static int tile13_lt() { return env_int("MQ_TILE13_LT", 8, 8, 9); }
 // passengers (256-byte runs, one tile buffer) instead of a 12-bit one
 // (fused config layer at 27 qubits 1.94 -> 1.87 ms, at 30 qubits 15.6 -> 15.5 ms).
 static bool euler_hi13() { return env_int("MQ_EULER_HI13", 1, 0, 1) == 1; }
+// Euler layers: the high bit group (1 = the lowest) whose sweep carries the
+// pre diagonal
+static int euler_pre_group() { return env_int("MQ_EULER_PRE_GROUP", 1, 1, 8); }
 
 // Register phases: targets (tile-local) chunked in the given order into
 // groups of LR; the last group is padded with the highest tile bits it does
@@ -1303,9 +1306,12 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
   Sweep first;
   std::vector<int> first_phase, first_rk;
   EpiPlan e_first;
+  // the high sweeps commute (disjoint qubits): the one that carries the pre
+  // diagonal runs first, the others follow in order
+  const size_t pre_g = groups.size() > 1 ? (size_t)std::min<int>(euler_pre_group(), (int)groups.size() - 1) : 0;
   const bool has_high = groups.size() > 1 &&
-                        build_u2_sweep(h, ry.data(), nullptr, groups[1].first, groups[1].second, first, first_phase,
-                                       first_rk, nullptr, hi_tmin(groups[1].second));
+                        build_u2_sweep(h, ry.data(), nullptr, groups[pre_g].first, groups[pre_g].second, first,
+                                       first_phase, first_rk, nullptr, hi_tmin(groups[pre_g].second));
   first.rot = rot;
   {
     const Sweep& fs = has_high ? first : low;
@@ -1334,19 +1340,19 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
     }
   }
   *done = true;
+  if (has_high) {
+    int rc = run_sweep(h, first, first_phase, first_rk, &e_first);
+    if (rc) return rc;
+  }
   for (size_t g = 1; g < groups.size(); ++g) {
-    int rc;
-    if (g == 1) {
-      rc = run_sweep(h, first, first_phase, first_rk, &e_first);
-    } else {
-      Sweep sw;
-      std::vector<int> op_phase, op_rk;
-      if (!build_u2_sweep(h, ry.data(), nullptr, groups[g].first, groups[g].second, sw, op_phase, op_rk, nullptr,
-                          hi_tmin(groups[g].second)))
-        continue;
-      sw.rot = rot;
-      rc = run_sweep(h, sw, op_phase, op_rk);
-    }
+    if (g == pre_g) continue;
+    Sweep sw;
+    std::vector<int> op_phase, op_rk;
+    if (!build_u2_sweep(h, ry.data(), nullptr, groups[g].first, groups[g].second, sw, op_phase, op_rk, nullptr,
+                        hi_tmin(groups[g].second)))
+      continue;
+    sw.rot = rot;
+    int rc = run_sweep(h, sw, op_phase, op_rk);
     if (rc) return rc;
   }
   int rc = run_sweep(h, low, low_phase, low_rk, &e);
