@@ -55,6 +55,8 @@ def parse_args():
     ap.add_argument("--cpu-qubits", type=int, default=int(os.environ.get("MQ_BENCH_CPU_QUBITS", "28")))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-infidelity", action="store_true",
+                    help="skip the complex128 run of the scale circuit (1 - |<psi64|psi128>|^2)")
     return ap.parse_args()
 
 
@@ -204,6 +206,37 @@ def cpu_baseline_sample(n_target: int, n_cpu: int, circuit, repeats: int = 1, th
     return total, sample, T
 
 
+# ---------------------------------------------------------------- fidelity
+class _DeviceArray:
+    """A device buffer of n complex amplitudes as a __cuda_array_interface__
+    object (torch.as_tensor wraps it without a copy)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False),
+                                         "strides": None, "version": 3}
+
+
+def infidelity_vs_c128(sv64, sv128, device) -> float:
+    """1 - |<psi64|psi128>|^2 / (<psi64|psi64> <psi128|psi128>) of two device
+    states, summed in complex128 on the GPU in chunks of 2^26 amplitudes."""
+    import torch
+    n = 1 << sv64.n
+    a = torch.as_tensor(_DeviceArray(sv64.device_ptr(), n, "<c8"), device=device)
+    b = torch.as_tensor(_DeviceArray(sv128.device_ptr(), n, "<c16"), device=device)
+    ov = torch.zeros((), dtype=torch.complex128, device=device)
+    na = torch.zeros((), dtype=torch.float64, device=device)
+    nb = torch.zeros((), dtype=torch.float64, device=device)
+    step = 1 << 26
+    for s in range(0, n, step):
+        x = a[s:s + step].to(torch.complex128)
+        y = b[s:s + step]
+        ov += torch.vdot(x, y)
+        na += torch.vdot(x, x).real
+        nb += torch.vdot(y, y).real
+    f = (ov.abs() ** 2 / (na * nb)).item()
+    return max(0.0, 1.0 - f)
+
+
 # ---------------------------------------------------------------- our arm
 def run_ours(args, rank, world, local_rank, dist):
     import torch
@@ -279,6 +312,15 @@ def run_ours(args, rank, world, local_rank, dist):
     launches = c1[0] - c0[0]
     sweeps = c1[1] - c0[1]
 
+    # accuracy of the timed result (untimed): the same circuit in complex128
+    infid = None
+    if not args.no_infidelity:
+        sv128 = StateVector(n, "complex128", device=local_rank, stream=stream.cuda_stream)
+        W.run_circuit_layers(sv128, circuit)
+        torch.cuda.synchronize()
+        infid = infidelity_vs_c128(sv, sv128, f"cuda:{local_rank}")
+        sv128.close()
+
     value = world * args.steps * logical * layer_bytes / elapsed / 1e9
     peak, peak_kind = measured_peaks()
     # dominant kernel: the tile sweep of the fused config layers (every launch
@@ -327,6 +369,7 @@ def run_ours(args, rank, world, local_rank, dist):
                    "parallelism": f"replicas x{world}"},
         "layer_breakdown": breakdown,
         "sweeps_per_step": sweeps / args.steps,
+        "infidelity_vs_c128": infid,
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": "k_tile (sweep of the fused U(2)+RZZ+CNOT-ladder layer)",
                      "achieved": achieved, "peak": peak,
