@@ -1,0 +1,85 @@
+"""The workload configurations as parity cases, through the public API.
+
+* Plain statevector, 20 qubits, complex64, seed 0: 20 layers of [Haar U(2)
+  on every qubit, RZZ(i, i+1) with angles U[0, 2pi), CNOT ladder], the full
+  probability vector and 1000 seeded shots.  The CPU oracle (the reference's
+  per-gate algorithm, complex128) runs it in full: amplitudes within 1e-5,
+  probabilities within 1e-6, shots bit-exact with the oracle's stream on the
+  device's own probabilities.
+* Plain statevector at scale, 30 qubits: too large for the oracle, so a
+  size-independent property checks it: the complex64 state against the same
+  circuit run in complex128 on the GPU (infidelity <= 1e-9) and its norm.
+"""
+import numpy as np
+import pytest
+
+from oracle import OracleSim
+from oracle import sampler as osamp
+
+pytestmark = pytest.mark.gpu
+
+
+def test_plain_config_20_qubits_against_the_oracle():
+    from mettleq_b200 import workloads as W
+    from mettleq_b200.device import Device
+    from mettleq_b200.integrations import _common as C
+    n = 20
+    circ = W.plain_circuit(n, 20, seed=0)
+    ops, gphase = circ.ops()
+    dev = Device(n)
+    dev.execute(ops)
+    C.apply_global_phase(dev, gphase)
+    got = dev.statevector()
+    o = OracleSim(n, np.complex128)
+    o.execute(ops)
+    o.apply_global_phase(gphase)
+    assert float(np.max(np.abs(got.astype(np.complex128) - o.state))) <= 1e-5
+    probs = dev.sim.probabilities()
+    assert float(np.max(np.abs(probs - np.abs(o.state) ** 2))) <= 1e-6
+    idx = dev.sim.sample_indices(1000, seed=0)
+    assert np.array_equal(idx, osamp.sample_indices(osamp.amp2(got), 0, 1000))
+    dev.close()
+
+
+def _device_infidelity(sv64, sv128):
+    """(1 - |<a|b>|^2 / (<a|a><b|b>), <a|a>) of two device states, summed on the GPU
+    in complex128 (the 30-qubit states stay in device memory)."""
+    import torch
+
+    class _Dev:
+        def __init__(self, ptr, n, typestr):
+            self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False),
+                                             "strides": None, "version": 3}
+
+    n = 1 << sv64.n
+    sv64.synchronize()
+    sv128.synchronize()
+    a = torch.as_tensor(_Dev(sv64.device_ptr(), n, "<c8"), device="cuda:0")
+    b = torch.as_tensor(_Dev(sv128.device_ptr(), n, "<c16"), device="cuda:0")
+    ov = torch.zeros((), dtype=torch.complex128, device="cuda:0")
+    na = torch.zeros((), dtype=torch.float64, device="cuda:0")
+    nb = torch.zeros((), dtype=torch.float64, device="cuda:0")
+    for s in range(0, n, 1 << 26):
+        x = a[s:s + (1 << 26)].to(torch.complex128)
+        y = b[s:s + (1 << 26)]
+        ov += torch.vdot(x, y)
+        na += torch.vdot(x, x).real
+        nb += torch.vdot(y, y).real
+    torch.cuda.synchronize()
+    return 1.0 - (ov.abs() ** 2 / (na * nb)).item(), na.item()
+
+
+def test_scale_config_30_qubits_against_complex128():
+    from mettleq_b200 import workloads as W
+    from mettleq_b200.engine import StateVector
+    n = 30
+    circ = W.scale_circuit(n, 6, seed=0, qft_every=3)  # 6 config layers, 2 QFT + 2 GF(2) layers
+    sv64 = StateVector(n, "complex64")
+    sv128 = StateVector(n, "complex128")
+    W.run_circuit_layers(sv64, circ)
+    W.run_circuit_layers(sv128, circ)
+    infid, norm64 = _device_infidelity(sv64, sv128)
+    sv64.close()
+    sv128.close()
+    assert abs(1.0 - norm64) <= 1e-5
+    assert infid <= 1e-9
