@@ -411,6 +411,9 @@ __device__ __forceinline__ void apply_regdiag(V2<R> (&a)[16], const V2<R>* lut, 
 #ifndef MQ_MODE2_CTAS
 #define MQ_MODE2_CTAS 3
 #endif
+#ifndef MQ_LATE_PREFETCH
+#define MQ_LATE_PREFETCH 1
+#endif
 // Tile of 2^M amplitudes, 2^LT threads, 2^LR amplitudes per register
 // group.  Global traffic moves in 16-byte chunks (two complex64 or one
 // complex128 amplitude): chunk c covers tile-local element c << CB.
@@ -557,21 +560,33 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
     if (tile < P.n_tiles) load_tile(tile, bufs);
     cp_async_commit();
   }
+  // two buffers: the next tile is requested after the barrier that follows
+  // this tile's arrival; every thread has then finished the previous tile's
+  // write-back from the buffer it goes into, so the write-back needs no
+  // barrier of its own (three barriers per tile of two phases, not four)
+  constexpr bool LATE = NBUF == 2 && MQ_LATE_PREFETCH;
   T a[NR];
   for (int it = 0; tile < P.n_tiles; tile += gridDim.x, ++it) {
     T* cur = bufs + (NBUF == 2 ? (it & 1) * E : 0);
-    if constexpr (NBUF == 2) {
+    if constexpr (LATE) {
+      cp_async_wait<0>();
+      __syncthreads();
+      const uint32_t next = tile + gridDim.x;
+      if (next < P.n_tiles) load_tile(next, bufs + ((it + 1) & 1) * E);
+      cp_async_commit();
+    } else if constexpr (NBUF == 2) {
       const uint32_t next = tile + gridDim.x;
       if (next < P.n_tiles) load_tile(next, bufs + ((it + 1) & 1) * E);
       cp_async_commit();
       cp_async_wait<1>();
+      __syncthreads();
     } else {
       // the buffer is free: the previous tile's write-back ended with a barrier
       load_tile(tile, bufs);
       cp_async_commit();
       cp_async_wait<0>();
+      __syncthreads();
     }
-    __syncthreads();
     uint32_t cl_in;
     const uint32_t base = src_base(tile, cl_in);
     for (int ph = 0; ph < P.n_phases; ++ph) {
@@ -657,7 +672,7 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
     if constexpr (STORE_EPI) {
       if (P.epi.perm || P.epi.diag) {
         epilogue_store<R, M, LT, CPT>(P.epi, cur, ecols, elut, dst, tile << M, base, cl_in, tid, epi_ak);
-        __syncthreads();
+        if constexpr (!LATE) __syncthreads();
         continue;
       }
     }
@@ -678,7 +693,7 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
       }
       *reinterpret_cast<float4*>(dst + (gb | g_k(k))) = v;
     }
-    __syncthreads();
+    if constexpr (!LATE) __syncthreads();
   }
   cp_async_wait<0>();
 }
