@@ -408,6 +408,10 @@ __device__ __forceinline__ void apply_regdiag(V2<R> (&a)[16], const V2<R>* lut, 
   for (int r = 0; r < 16; ++r) a[r] = cmul(a[r], cmul(f, tr[r]));
 }
 
+// Build-time choices kept for comparison builds (-D...): resident CTAs per SM
+// of the 256-thread MODE 2 sweep (3: 80 registers a thread, the fused layer's
+// low sweep 0.5 ms faster at 30 qubits than with 2), and the late request of
+// the next tile (see k_tile; 0 requests it before waiting for the current one).
 #ifndef MQ_MODE2_CTAS
 #define MQ_MODE2_CTAS 3
 #endif
@@ -451,7 +455,6 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   T* bufs = reinterpret_cast<T*>(smem_raw);
   PhaseDesc* phs = reinterpret_cast<PhaseDesc*>(smem_raw + NBUF * sizeof(T) * E);
   const float2* tw = nullptr;
-  // MODE 2: permutation columns, then the diagonal tables
   // shared memory: tile buffers, the launch's phase descriptors, then (MODE
   // >= 2) the permutation columns and the diagonal tables
   const size_t ph_end = NBUF * sizeof(T) * E + sizeof(PhaseDesc) * P.n_phases;
@@ -761,11 +764,11 @@ static bool euler_hi13() { return env_int("MQ_EULER_HI13", 1, 0, 1) == 1; }
 static int euler_pre_group() { return env_int("MQ_EULER_PRE_GROUP", 1, 1, 8); }
 
 // Register phases: targets (tile-local) chunked in the given order into
-// groups of LR; the last group is padded with the highest tile bits it does
-// not hold (targets of other phases included: a slot without a gate is left
-// alone), which keeps tile bits 0-3 as thread bits and shared-memory access
-// free of bank conflicts.  Records the phase index and register slot of
-// every target.
+// groups of LR; the short group (the last, or with pad_first the first) is
+// padded with the highest tile bits it does not hold (targets of other phases
+// included: a slot without a gate is left alone), which keeps tile bits 0-3
+// as thread bits and shared-memory access free of bank conflicts.  Records
+// the phase index and register slot of every target.
 static void make_phases(int m, int lr, const std::vector<int>& order, Sweep& sw, std::vector<int>& op_phase,
                         std::vector<int>& op_rk, bool pad_first = false) {
   sw.phases.clear();
