@@ -125,8 +125,10 @@ struct Term {
 struct PlannedLut {
   std::vector<int> pos;  // index bit k of the table <- global bit pos[k]
   bool contig = false;
-  std::vector<std::complex<double>> vals;
+  std::vector<const Term*> members;          // terms the table holds
+  std::vector<std::complex<double>> vals;    // filled by realize() once a plan is chosen
 };
+static size_t lut_size(const PlannedLut& L) { return L.vals.empty() ? (size_t(1) << L.pos.size()) : L.vals.size(); }
 
 static std::complex<double> cis(double t) { return {std::cos(t), std::sin(t)}; }
 
@@ -178,14 +180,32 @@ static std::complex<double> term_value(const Term& tm, const std::vector<int>& p
   return tm.tab[idx];
 }
 
-static void finalize_lut(PlannedLut& L, const std::vector<const Term*>& members) {
+static void finalize_lut(PlannedLut& L) {
   const uint32_t sz = 1u << L.pos.size();
+  // table-local position of every member bit, found once
+  struct Local { int k, lp[2]; const std::complex<double>* tab; };
+  std::vector<Local> ms;
+  for (const Term* tm : L.members) {
+    Local m{(int)tm->bits.size(), {0, 0}, tm->tab.data()};
+    for (int j = 0; j < m.k; ++j)
+      m.lp[j] = (int)(std::find(L.pos.begin(), L.pos.end(), tm->bits[j]) - L.pos.begin());
+    ms.push_back(m);
+  }
   L.vals.assign(sz, 1.0);
   for (uint32_t x = 0; x < sz; ++x) {
     std::complex<double> v = 1.0;
-    for (const Term* tm : members) v *= term_value(*tm, L.pos, x);
+    for (const Local& m : ms) {
+      uint32_t idx = 0;
+      for (int j = 0; j < m.k; ++j) idx |= ((x >> m.lp[j]) & 1u) << (m.k - 1 - j);
+      v *= m.tab[idx];
+    }
     L.vals[x] = v;
   }
+}
+// Table values of a chosen plan (planning itself only sizes the tables).
+static void realize(std::vector<PlannedLut>& luts) {
+  for (auto& L : luts)
+    if (L.vals.empty()) finalize_lut(L);
 }
 
 // Greedy factorisation with windows of width <= W.
@@ -212,7 +232,7 @@ static std::vector<PlannedLut> plan_luts(const std::vector<Term>& terms, int W) 
     PlannedLut L;
     for (int b = s; b <= hi; ++b) L.pos.push_back(b);
     L.contig = true;
-    finalize_lut(L, members);
+    L.members = std::move(members);
     luts.push_back(std::move(L));
   }
   // far pairs: scattered-bit tables
@@ -233,7 +253,7 @@ static std::vector<PlannedLut> plan_luts(const std::vector<Term>& terms, int W) 
     L.contig = true;
     for (size_t k = 1; k < L.pos.size(); ++k)
       if (L.pos[k] != L.pos[0] + (int)k) L.contig = false;
-    finalize_lut(L, members);
+    L.members = std::move(members);
     luts.push_back(std::move(L));
   }
   return luts;
@@ -298,7 +318,7 @@ int plan_diag_windows(mq_state* h, int n_terms, const int32_t* kinds, const int3
     size_t entries = 0;
     bool contig = true;
     for (auto& L : luts) {
-      entries += L.vals.size();
+      entries += lut_size(L);
       contig = contig && L.contig && !L.pos.empty();
     }
     if (!contig || (int)luts.size() > kMaxLuts) continue;
@@ -311,6 +331,7 @@ int plan_diag_windows(mq_state* h, int n_terms, const int32_t* kinds, const int3
       entries = 2;
     }
     if ((int)entries > max_entries) continue;
+    realize(luts);
     for (auto& v : luts[0].vals) v *= scalar;
     out.n = (int)luts.size();
     uint32_t off = 0;
@@ -371,12 +392,13 @@ int plan_diag_register(mq_state* h, int n_terms, const int32_t* kinds, const int
     size_t entries = (nt / 16) * 17;
     bool contig = true;
     for (auto& L : luts) {
-      entries += L.vals.size();
+      entries += lut_size(L);
       contig = contig && L.contig && !L.pos.empty();
     }
     ok = contig && (int)luts.size() <= kMaxLuts && (int)entries <= max_entries;
   }
   if (!ok) return MQ_OK;
+  realize(luts);
   out.nc = (int)cross.size();
   for (int j = 0; j < out.nc; ++j) out.cbit[j] = cross[j];
   out.win.n = (int)luts.size();
@@ -416,7 +438,7 @@ int launch_diag_terms(mq_state* h, int n_terms, const int32_t* kinds, const int3
   for (int W = 10; W >= 1; --W) {
     luts = plan_luts(terms, W);
     size_t entries = 0;
-    for (auto& L : luts) entries += L.vals.size();
+    for (auto& L : luts) entries += lut_size(L);
     if ((int)luts.size() <= kMaxLuts && (int)entries <= cap) break;
     if (W == 1) break;  // fall through to multi-pass below
   }
@@ -426,6 +448,7 @@ int launch_diag_terms(mq_state* h, int n_terms, const int32_t* kinds, const int3
     L.vals = {1.0};
     luts.push_back(L);
   }
+  realize(luts);
   for (auto& v : luts[0].vals) v *= scalar;
   // Split into passes that respect the parameter-block capacity.
   size_t i = 0;
