@@ -34,7 +34,13 @@ struct PermParams {
   uint32_t lin_in[16];
   uint32_t lin_out[16];
   uint32_t tab[16];
+  // coset offsets of tile t as XORs of byte tables: h_in(t) = c ^ XOR_k
+  // hin[k][byte k of t], h_out likewise (read at CTA-uniform indices)
+  uint32_t hin[4][256];
+  uint32_t hout[4][256];
 };
+
+static_assert(sizeof(PermParams) <= 32000, "kernel parameter block too large");
 
 // Persistent CTAs stream cosets through two shared-memory buffers: the input
 // coset of tile t+grid is fetched with cp.async while tile t is written out.
@@ -64,15 +70,14 @@ __global__ void __launch_bounds__(256) k_perm(const V2<R>* __restrict__ in, V2<R
     t_in[e] = a; t_out[e] = b; t_tab[e] = c;
   }
   __syncthreads();
-  auto h_of = [&](uint32_t tile, bool input) -> uint32_t {
-    uint32_t h = input ? P.c : 0u;
-    for (int k = 0; k < P.n_comp; ++k)
-      if ((tile >> k) & 1u) h ^= input ? P.comp_in[k] : P.comp_out[k];
-    return h;
+  auto h_in_of = [&](uint32_t t) -> uint32_t {
+    return P.c ^ P.hin[0][t & 255u] ^ P.hin[1][(t >> 8) & 255u] ^ P.hin[2][(t >> 16) & 255u] ^ P.hin[3][t >> 24];
+  };
+  auto h_out_of = [&](uint32_t t) -> uint32_t {
+    return P.hout[0][t & 255u] ^ P.hout[1][(t >> 8) & 255u] ^ P.hout[2][(t >> 16) & 255u] ^ P.hout[3][t >> 24];
   };
   // per-thread parts: input chunks c = tid + NT*j cover elements 2c, 2c+1
-  auto issue = [&](uint32_t tile, int which) {
-    const uint32_t h_in = h_of(tile, true);
+  auto issue = [&](uint32_t h_in, int which) {
     const uint32_t sb = smem_u32(&buf[which][0]);
     if constexpr (PAIRS) {
 #pragma unroll
@@ -92,17 +97,20 @@ __global__ void __launch_bounds__(256) k_perm(const V2<R>* __restrict__ in, V2<R
     }
   };
   uint32_t tile = blockIdx.x;
-  if (tile < P.n_tiles) issue(tile, 0);
+  uint32_t h_cur = tile < P.n_tiles ? h_in_of(tile) : 0u;
+  if (tile < P.n_tiles) issue(h_cur, 0);
   cp_async_commit();
   for (int it = 0; tile < P.n_tiles; tile += gridDim.x, ++it) {
     const uint32_t next = tile + gridDim.x;
-    if (next < P.n_tiles) issue(next, (it + 1) & 1);
+    const uint32_t h_next = next < P.n_tiles ? h_in_of(next) : 0u;
+    if (next < P.n_tiles) issue(h_next, (it + 1) & 1);
     cp_async_commit();
     cp_async_wait<1>();
     __syncthreads();
     const T* cb = buf[it & 1];
-    const uint32_t h_out = h_of(tile, false);
-    const uint32_t flip = PAIRS ? (h_of(tile, true) & 1u) : 0u;
+    const uint32_t h_out = h_out_of(tile);
+    const uint32_t flip = PAIRS ? (h_cur & 1u) : 0u;
+    h_cur = h_next;
 #pragma unroll
     for (int j = 0; j < EPT; ++j) {
       const uint32_t e = (uint32_t)tid + (uint32_t)(NT * j);
@@ -279,6 +287,14 @@ int launch_affine_cols(mq_state* h, const uint32_t* cols, uint32_t c) {
   if (nc != n - D) return fail(MQ_EDEVICE, "affine coset basis construction failed");
   P.n_comp = (uint8_t)nc;
   P.n_tiles = 1u << nc;
+  for (int k = 0; k < 4; ++k)
+    for (uint32_t x = 0; x < 256; ++x) {
+      uint32_t a = 0, b = 0;
+      for (int bit = 0; bit < 8; ++bit)
+        if (((x >> bit) & 1u) && 8 * k + bit < nc) { a ^= P.comp_in[8 * k + bit]; b ^= P.comp_out[8 * k + bit]; }
+      P.hin[k][x] = a;
+      P.hout[k][x] = b;
+    }
   return h->dtype == MQ_C64 ? launch_perm_t<float>(h, P) : launch_perm_t<double>(h, P);
 }
 
