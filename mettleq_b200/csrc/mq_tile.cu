@@ -280,48 +280,60 @@ __device__ __forceinline__ void apply_u2_phase(V2<R> (&a)[1 << LR], const PhaseD
 // Twiddle per group), Lr from the register bits, whose factor treg[r] the
 // host tabulates per stage, so a pair costs one complex product for its
 // phase.
-template <typename R, int LR, int K>
+template <typename R, int LR, int K, bool FWD>
 __device__ __forceinline__ void apply_qft(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const V2<R>* treg,
                                           const float2* tw) {
   using T = V2<R>;
   constexpr int NR = 1 << LR;
   const int width = op.width;
-  const bool fwd = op.kind == OP_QFT_FWD;
-  T tg = mk<R>(1, 0);
-  if (width) {
-    const uint32_t mask = (width >= 32) ? 0xffffffffu : ((1u << width) - 1u);
-    const uint32_t Lg = (gq >> op.lad_shift) & mask;
-    if (Lg) tg = Twiddle<R>::get(tw, Lg, width);
+  if (width == 0) {  // the first stage of a register: no ladder bits, no phase
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      if (r & (1 << K)) continue;
+      const T x0 = a[r], x1 = a[r | (1 << K)];
+      a[r] = cadd(x0, x1);
+      a[r | (1 << K)] = csub(x0, x1);
+    }
+    return;
   }
+  // Lg = 0 reads entry 0 of every twiddle table, exactly 1
+  const uint32_t mask = (width >= 32) ? 0xffffffffu : ((1u << width) - 1u);
+  const T tg = Twiddle<R>::get(tw, (gq >> op.lad_shift) & mask, width);
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
     if (r & (1 << K)) continue;
     const int r1 = r | (1 << K);
     T x0 = a[r], x1 = a[r1];
-    if (fwd) {
-      T d = csub(x0, x1);
+    const T w = cmul(tg, treg[r1]);
+    if constexpr (FWD) {
       a[r] = cadd(x0, x1);
-      if (width) d = cmul(d, cmul(tg, treg[r1]));
-      a[r1] = d;
+      a[r1] = cmul(csub(x0, x1), w);
     } else {
-      if (width) x1 = cmulc(x1, cmul(tg, treg[r1]));
+      x1 = cmulc(x1, w);
       a[r] = cadd(x0, x1);
       a[r1] = csub(x0, x1);
     }
   }
 }
 
+template <typename R, int LR, bool FWD>
+__device__ __forceinline__ void apply_qft_dir(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const V2<R>* treg,
+                                              const float2* tw) {
+  switch (op.rk) {
+    case 0: apply_qft<R, LR, 0, FWD>(a, op, gq, treg, tw); break;
+    case 1: if constexpr (LR > 1) apply_qft<R, LR, 1, FWD>(a, op, gq, treg, tw); break;
+    case 2: if constexpr (LR > 2) apply_qft<R, LR, 2, FWD>(a, op, gq, treg, tw); break;
+    case 3: if constexpr (LR > 3) apply_qft<R, LR, 3, FWD>(a, op, gq, treg, tw); break;
+    case 4: if constexpr (LR > 4) apply_qft<R, LR, 4, FWD>(a, op, gq, treg, tw); break;
+    default: break;
+  }
+}
+
 template <typename R, int LR>
 __device__ __forceinline__ void apply_qft_op(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const V2<R>* treg,
                                              const float2* tw) {
-  switch (op.rk) {
-    case 0: apply_qft<R, LR, 0>(a, op, gq, treg, tw); break;
-    case 1: if constexpr (LR > 1) apply_qft<R, LR, 1>(a, op, gq, treg, tw); break;
-    case 2: if constexpr (LR > 2) apply_qft<R, LR, 2>(a, op, gq, treg, tw); break;
-    case 3: if constexpr (LR > 3) apply_qft<R, LR, 3>(a, op, gq, treg, tw); break;
-    case 4: if constexpr (LR > 4) apply_qft<R, LR, 4>(a, op, gq, treg, tw); break;
-    default: break;
-  }
+  if (op.kind == OP_QFT_FWD) apply_qft_dir<R, LR, true>(a, op, gq, treg, tw);
+  else apply_qft_dir<R, LR, false>(a, op, gq, treg, tw);
 }
 
 // Shared-memory slot of tile-local amplitude i (the chunk swizzle of k_tile
@@ -459,6 +471,7 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   // >= 2) the permutation columns and the diagonal tables
   const size_t ph_end = NBUF * sizeof(T) * E + sizeof(PhaseDesc) * P.n_phases;
   uint32_t* ecols = reinterpret_cast<uint32_t*>(smem_raw + ph_end);
+  T* qreg = reinterpret_cast<T*>(smem_raw + ph_end);  // MODE 1: per op, the register factors treg[32]
   T* elut = reinterpret_cast<T*>(smem_raw + ph_end + 128);
   const int tid = threadIdx.x;
   {
@@ -480,6 +493,14 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
         }
       }
     }
+  }
+  if constexpr (QFT) {
+    const uint32_t words = (uint32_t)P.n_ops * 32u * (uint32_t)(sizeof(T) / 4);
+    const uint32_t* srcw;
+    if constexpr (sizeof(R) == 4) srcw = reinterpret_cast<const uint32_t*>(&P.twf[0][0]);
+    else srcw = reinterpret_cast<const uint32_t*>(&P.twd[0][0]);
+    uint32_t* dstw = reinterpret_cast<uint32_t*>(qreg);
+    for (uint32_t w = tid; w < words; w += NT) dstw[w] = srcw[w];
   }
   if constexpr (EPI) {
     for (int w = tid; w < 32; w += NT) ecols[w] = P.epi.cols[w];
@@ -633,12 +654,7 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
           if (P.epi.pre.on && ph == 0) apply_regdiag<R>(a, elut, P.epi.pre, gq);
         }
         if constexpr (QFT) {
-          for (int o = P.ph_op[ph]; o < P.ph_op[ph + 1]; ++o) {
-            const V2<R>* treg;
-            if constexpr (sizeof(R) == 4) treg = P.twf[o];
-            else treg = P.twd[o];
-            apply_qft_op<R, LR>(a, P.ops[o], gq, treg, tw);
-          }
+          for (int o = P.ph_op[ph]; o < P.ph_op[ph + 1]; ++o) apply_qft_op<R, LR>(a, P.ops[o], gq, qreg + 32 * o, tw);
         } else {
           if (D.any_ctl) apply_u2_phase<R, LR, true, (MODE < 2)>(a, D, gq, greg);
           else apply_u2_phase<R, LR, false, (MODE < 2)>(a, D, gq, greg);
@@ -1129,6 +1145,7 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
         Q.twd[w][r] = make_double2(c, sn);
       }
     }
+    smem += (size_t)P.n_ops * 32 * h->amp_bytes();  // the register factors, staged in shared memory
     if (h->dtype == MQ_C64) return dispatch_tile<float, 1>(h, Q, smem, false);
     return dispatch_tile<double, 1>(h, Q, smem, false);
   }
