@@ -299,12 +299,23 @@ __device__ __forceinline__ void apply_qft(V2<R> (&a)[1 << LR], const TileOp& op,
   // Lg = 0 reads entry 0 of every twiddle table, exactly 1
   const uint32_t mask = (width >= 32) ? 0xffffffffu : ((1u << width) - 1u);
   const T tg = Twiddle<R>::get(tw, (gq >> op.lad_shift) & mask, width);
+  // a pair's register factor depends only on the register bits below K (the
+  // bits above the stage's bit are not ladder bits): for K < 3 the 2^K
+  // distinct products are formed once
+  constexpr int NW = K < 3 ? (1 << K) : 1;
+  T wk[NW];
+  if constexpr (K < 3) {
+#pragma unroll
+    for (int j = 0; j < NW; ++j) wk[j] = cmul(tg, treg[j | (1 << K)]);
+  }
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
     if (r & (1 << K)) continue;
     const int r1 = r | (1 << K);
     T x0 = a[r], x1 = a[r1];
-    const T w = cmul(tg, treg[r1]);
+    T w;
+    if constexpr (K < 3) w = wk[r & (NW - 1)];
+    else w = cmul(tg, treg[r1]);
     if constexpr (FWD) {
       a[r] = cadd(x0, x1);
       a[r1] = cmul(csub(x0, x1), w);
@@ -1143,6 +1154,14 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
         const double c = std::cos(ang), sn = std::sin(ang);
         Q.twf[w][r] = make_float2((float)c, (float)sn);
         Q.twd[w][r] = make_double2(c, sn);
+      }
+      // the kernel forms a pair's factor from its register bits below the
+      // stage's slot only
+      const int K = op.rk;
+      for (int r = 0; r < (1 << lr); ++r) {
+        const int r0 = (r & ((1 << K) - 1)) | (1 << K);
+        if (((r >> K) & 1) && (Q.twd[w][r].x != Q.twd[w][r0].x || Q.twd[w][r].y != Q.twd[w][r0].y))
+          return fail(MQ_EINVAL, "QFT stage with a ladder bit above its own bit");
       }
     }
     smem += (size_t)P.n_ops * 32 * h->amp_bytes();  // the register factors, staged in shared memory
