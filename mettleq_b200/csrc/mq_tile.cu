@@ -91,6 +91,7 @@ struct TileParams {
   BaseRuns runs;  // tile index -> base index (deposit_runs)
   double scale;
   uint8_t ph_op[kMaxPhases + 2];     // QFT: ops of phase p are [ph_op[p], ph_op[p+1])
+  uint8_t qchain[kMaxPhases];        // QFT: 1 + the largest width when the phase's stages chain (else 0)
   // U(2) matrices read from device memory at launch (mats_dev[8 q ..]):
   // slot k of phase p takes row mat_q[p][k] - 1 (0 = the matrix in ph)
   int16_t mat_q[kMaxPhases][5];
@@ -281,8 +282,7 @@ __device__ __forceinline__ void apply_u2_phase(V2<R> (&a)[1 << LR], const PhaseD
 // host tabulates per stage, so a pair costs one complex product for its
 // phase.
 template <typename R, int LR, int K, bool FWD>
-__device__ __forceinline__ void apply_qft(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const V2<R>* treg,
-                                          const float2* tw) {
+__device__ __forceinline__ void apply_qft(V2<R> (&a)[1 << LR], const TileOp& op, V2<R> tg, const V2<R>* treg) {
   using T = V2<R>;
   constexpr int NR = 1 << LR;
   const int width = op.width;
@@ -296,9 +296,6 @@ __device__ __forceinline__ void apply_qft(V2<R> (&a)[1 << LR], const TileOp& op,
     }
     return;
   }
-  // Lg = 0 reads entry 0 of every twiddle table, exactly 1
-  const uint32_t mask = (width >= 32) ? 0xffffffffu : ((1u << width) - 1u);
-  const T tg = Twiddle<R>::get(tw, (gq >> op.lad_shift) & mask, width);
   // a pair's register factor depends only on the register bits below K (the
   // bits above the stage's bit are not ladder bits): for K < 3 the 2^K
   // distinct products are formed once
@@ -328,23 +325,32 @@ __device__ __forceinline__ void apply_qft(V2<R> (&a)[1 << LR], const TileOp& op,
 }
 
 template <typename R, int LR, bool FWD>
-__device__ __forceinline__ void apply_qft_dir(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const V2<R>* treg,
-                                              const float2* tw) {
+__device__ __forceinline__ void apply_qft_dir(V2<R> (&a)[1 << LR], const TileOp& op, V2<R> tg, const V2<R>* treg) {
   switch (op.rk) {
-    case 0: apply_qft<R, LR, 0, FWD>(a, op, gq, treg, tw); break;
-    case 1: if constexpr (LR > 1) apply_qft<R, LR, 1, FWD>(a, op, gq, treg, tw); break;
-    case 2: if constexpr (LR > 2) apply_qft<R, LR, 2, FWD>(a, op, gq, treg, tw); break;
-    case 3: if constexpr (LR > 3) apply_qft<R, LR, 3, FWD>(a, op, gq, treg, tw); break;
-    case 4: if constexpr (LR > 4) apply_qft<R, LR, 4, FWD>(a, op, gq, treg, tw); break;
+    case 0: apply_qft<R, LR, 0, FWD>(a, op, tg, treg); break;
+    case 1: if constexpr (LR > 1) apply_qft<R, LR, 1, FWD>(a, op, tg, treg); break;
+    case 2: if constexpr (LR > 2) apply_qft<R, LR, 2, FWD>(a, op, tg, treg); break;
+    case 3: if constexpr (LR > 3) apply_qft<R, LR, 3, FWD>(a, op, tg, treg); break;
+    case 4: if constexpr (LR > 4) apply_qft<R, LR, 4, FWD>(a, op, tg, treg); break;
     default: break;
   }
 }
 
+// tg: the group factor e^{i pi Lg / 2^width} of the stage (1 for width 0)
 template <typename R, int LR>
-__device__ __forceinline__ void apply_qft_op(V2<R> (&a)[1 << LR], const TileOp& op, uint32_t gq, const V2<R>* treg,
-                                             const float2* tw) {
-  if (op.kind == OP_QFT_FWD) apply_qft_dir<R, LR, true>(a, op, gq, treg, tw);
-  else apply_qft_dir<R, LR, false>(a, op, gq, treg, tw);
+__device__ __forceinline__ void apply_qft_op(V2<R> (&a)[1 << LR], const TileOp& op, V2<R> tg, const V2<R>* treg) {
+  if (op.kind == OP_QFT_FWD) apply_qft_dir<R, LR, true>(a, op, tg, treg);
+  else apply_qft_dir<R, LR, false>(a, op, tg, treg);
+}
+
+// The group factor of a stage from the twiddle tables (Lg = 0 reads entry 0
+// of every table, exactly 1).
+template <typename R>
+__device__ __forceinline__ V2<R> qft_group_factor(const TileOp& op, uint32_t gq, const float2* tw) {
+  const int width = op.width;
+  if (width == 0) return mk<R>(1, 0);
+  const uint32_t mask = (width >= 32) ? 0xffffffffu : ((1u << width) - 1u);
+  return Twiddle<R>::get(tw, (gq >> op.lad_shift) & mask, width);
 }
 
 // Shared-memory slot of tile-local amplitude i (the chunk swizzle of k_tile
@@ -665,7 +671,33 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
           if (P.epi.pre.on && ph == 0) apply_regdiag<R>(a, elut, P.epi.pre, gq);
         }
         if constexpr (QFT) {
-          for (int o = P.ph_op[ph]; o < P.ph_op[ph + 1]; ++o) apply_qft_op<R, LR>(a, P.ops[o], gq, qreg + 32 * o, tw);
+          const int o0 = P.ph_op[ph], o1 = P.ph_op[ph + 1];
+          if (P.qchain[ph]) {
+            // the phase's stages sit on consecutive bits over one ladder, so
+            // they share Lg (the ladder bits below the phase) and differ in
+            // width by one: the factor of width w - d is p^(2^d), p the factor
+            // at the largest width w (squarings instead of table lookups)
+            const int wmax = P.qchain[ph] - 1;
+            T pw[LR];
+            pw[0] = mk<R>(1, 0);
+            if (wmax) {
+              const uint32_t mask = (wmax >= 32) ? 0xffffffffu : ((1u << wmax) - 1u);
+              pw[0] = Twiddle<R>::get(tw, (gq >> P.ops[o0].lad_shift) & mask, wmax);
+            }
+#pragma unroll
+            for (int d = 1; d < LR; ++d) pw[d] = cmul(pw[d - 1], pw[d - 1]);
+            for (int o = o0; o < o1; ++o) {
+              const int d = wmax - P.ops[o].width;
+              T tg = pw[0];
+#pragma unroll
+              for (int e = 1; e < LR; ++e)
+                if (d == e) tg = pw[e];
+              apply_qft_op<R, LR>(a, P.ops[o], tg, qreg + 32 * o);
+            }
+          } else {
+            for (int o = o0; o < o1; ++o)
+              apply_qft_op<R, LR>(a, P.ops[o], qft_group_factor<R>(P.ops[o], gq, tw), qreg + 32 * o);
+          }
         } else {
           if (D.any_ctl) apply_u2_phase<R, LR, true, (MODE < 2)>(a, D, gq, greg);
           else apply_u2_phase<R, LR, false, (MODE < 2)>(a, D, gq, greg);
@@ -1088,6 +1120,23 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
       }
     }
     P.ph_op[sw.phases.size()] = (uint8_t)w;
+    // chained phases: every stage's ladder is the bits from one lad_shift up
+    // to its own bit, and the stage bits are consecutive
+    for (size_t p = 0; p < sw.phases.size(); ++p) {
+      const int o0 = P.ph_op[p], o1 = P.ph_op[p + 1];
+      if (o1 <= o0) continue;
+      bool chain = true;
+      int wmax = 0, gmin = 64, gmax = -1;
+      for (int o = o0; o < o1 && chain; ++o) {
+        const TileOp& op = P.ops[o];
+        const int g = sw.tile_bits[sw.phases[p][op.rk]];
+        chain = op.lad_shift == P.ops[o0].lad_shift && op.width == g - (int)op.lad_shift;
+        wmax = std::max(wmax, (int)op.width);
+        gmin = std::min(gmin, g);
+        gmax = std::max(gmax, g);
+      }
+      if (chain && gmax - gmin == o1 - o0 - 1 && wmax <= 31) P.qchain[p] = (uint8_t)(wmax + 1);
+    }
   } else {
     for (size_t o = 0; o < sw.ops.size(); ++o) {
       PhaseDesc& D = P.ph[op_phase[o]];
