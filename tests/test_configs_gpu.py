@@ -9,6 +9,8 @@
 * Plain statevector at scale, 30 qubits: too large for the oracle, so a
   size-independent property checks it: the complex64 state against the same
   circuit run in complex128 on the GPU (infidelity <= 1e-9) and its norm.
+* Its random GF(2) layer at 28 qubits, bit-exact against the oracle's source
+  map evaluated on the GPU.
 """
 import numpy as np
 import pytest
@@ -83,3 +85,35 @@ def test_scale_config_30_qubits_against_complex128():
     sv128.close()
     assert abs(1.0 - norm64) <= 1e-5
     assert infid <= 1e-9
+
+
+def test_random_gf2_layer_28_qubits_bit_exact():
+    """A random invertible GF(2) layer at 28 qubits (2^18 cosets: every byte
+    table of the coset offsets in use) against an independent gather: the
+    oracle's source map src[y] = sum_k parity(rows[k] & y) << (n-1-k) ^ c
+    (oracle.affine_sources) evaluated on the GPU with torch, bit-exact."""
+    import torch
+    from mettleq_b200.engine import StateVector
+    from tests.helpers import random_invertible_rows
+    n = 28
+    rng = np.random.default_rng(2028)
+    rows = random_invertible_rows(n, rng)
+    c = int(rng.integers(0, 1 << n))
+    dev = torch.device("cuda:0")
+    gen = torch.Generator(device=dev).manual_seed(5)
+    vec = torch.complex(torch.randn(1 << n, generator=gen, device=dev),
+                        torch.randn(1 << n, generator=gen, device=dev)).to(torch.complex64)
+    sv = StateVector(n, "complex64")
+    sv.set(vec.cpu().numpy())
+    sv.apply_xor_affine(rows, c)
+    got = torch.from_numpy(sv.get()).to(dev)
+    sv.close()
+    y = torch.arange(1 << n, dtype=torch.int64, device=dev)
+    src = torch.zeros_like(y)
+    for k, r in enumerate(rows):
+        par = y & r
+        for sh in (16, 8, 4, 2, 1):
+            par = par ^ (par >> sh)
+        src |= (par & 1) << (n - 1 - k)
+    src ^= c
+    assert torch.equal(got, vec[src])
