@@ -11,7 +11,8 @@
   circuit run in complex128 on the GPU (infidelity <= 1e-9) and its norm.
 * Its random GF(2) layer at 28 qubits, bit-exact against the oracle's source
   map evaluated on the GPU; its fused config layer at 28 qubits against the
-  same layer as separate passes on other kernels.
+  same layer as separate passes on other kernels; its QFT at 28 qubits on
+  basis states against the closed form.
 """
 import numpy as np
 import pytest
@@ -155,3 +156,46 @@ def test_fused_layer_28_qubits_against_separate_layers():
     b = sep.get()
     sep.close()
     assert float(np.max(np.abs(a - b))) <= 1e-5
+
+
+def _bit_reverse(k, n):
+    r = k & 0
+    for i in range(n):
+        r = r | (((k >> i) & 1) << (n - 1 - i))
+    return r
+
+
+def test_qft_28_qubits_on_basis_states_closed_form():
+    """The 28-qubit QFT (no final swaps) of a basis state |x> against its
+    closed form out[k] = e^{2 pi i x rev(k) / 2^n} / 2^{n/2} (rev: n-bit
+    reversal), evaluated on the GPU in float64 from exact integer phases.
+    The closed form is first checked against the oracle's gate-by-gate QFT at
+    6 qubits.  Amplitudes within 2e-5 of their magnitude 2^{-n/2}."""
+    import torch
+    from mettleq_b200.engine import StateVector
+    m = 6
+    for x in (0, 1, 13, 63):
+        v = np.zeros(1 << m, np.complex128)
+        v[x] = 1.0
+        o = OracleSim(m, np.complex128)
+        o.set_state(v)
+        o.qft()
+        k = np.arange(1 << m)
+        ref = np.exp(2j * np.pi * x * _bit_reverse(k, m) / (1 << m)) / np.sqrt(1 << m)
+        assert float(np.max(np.abs(o.state - ref))) <= 1e-12
+    n = 28
+    dev = torch.device("cuda:0")
+    sv = StateVector(n, "complex64")
+    for x in (0x9E3779B & ((1 << n) - 1), (1 << n) - 1):
+        v = np.zeros(1 << n, np.complex64)
+        v[x] = 1.0
+        sv.set(v)
+        sv.apply_qft()
+        got = torch.from_numpy(sv.get()).to(dev)
+        k = torch.arange(1 << n, dtype=torch.int64, device=dev)
+        ph = (x * _bit_reverse(k, n)) % (1 << n)  # exact: x, rev(k) < 2^28
+        ang = ph.to(torch.float64) * (2.0 * np.pi / (1 << n))
+        ref = torch.polar(torch.full_like(ang, 2.0 ** (-n / 2)), ang)
+        err = (got.to(torch.complex128) - ref).abs().max().item()
+        assert err <= 2e-5 * 2.0 ** (-n / 2), err
+    sv.close()
