@@ -28,6 +28,18 @@ from oracle import sampler as osamp
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True)
+def _release_torch_cache():
+    """The full-size checks build references with torch on the device; hand
+    its cached blocks back after each test, so that later tests (which
+    allocate through libmq) find the memory free."""
+    yield
+    import torch
+    if torch.cuda.is_initialized():
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+
+
 def test_plain_config_20_qubits_against_the_oracle():
     from mettleq_b200 import workloads as W
     from mettleq_b200.device import Device
