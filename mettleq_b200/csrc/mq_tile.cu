@@ -818,6 +818,8 @@ static int tile13_lt() { return env_int("MQ_TILE13_LT", 8, 8, 9); }
 // passengers (256-byte runs, one tile buffer) instead of a 12-bit one
 // (fused config layer at 27 qubits 1.94 -> 1.87 ms, at 30 qubits 15.6 -> 15.5 ms).
 static bool euler_hi13() { return env_int("MQ_EULER_HI13", 1, 0, 1) == 1; }
+// U(2) layers without diagonal terms through the Euler split as well.
+static bool euler_plain() { return env_int("MQ_EULER_PLAIN", 1, 0, 1) == 1; }
 // Euler layers: the high bit group (1 = the lowest) whose sweep carries the
 // pre diagonal
 static int euler_pre_group() { return env_int("MQ_EULER_PRE_GROUP", 1, 1, 8); }
@@ -1304,6 +1306,14 @@ static bool build_u2_sweep(mq_state* h, const double* mats, const uint8_t* activ
 }
 
 int launch_u2_layer(mq_state* h, const double* mats, const uint8_t* active) {
+  // a U(2) on every qubit takes the Euler split too (RY sweeps in tangent
+  // form between the two RZ diagonals)
+  if (euler_plain() && euler_enabled(h)) {
+    bool all = true;
+    if (active)
+      for (int q = 0; q < h->n; ++q) all = all && active[q];
+    if (all) return launch_layer(h, mats, nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0);
+  }
   for (auto [start, cnt] : split_bits(h->n, tile_max(h->dtype), passengers())) {
     Sweep sw;
     std::vector<int> op_phase, op_rk;
@@ -1481,9 +1491,9 @@ int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_t
     if (all) active = nullptr;
   }
   // the split pays when the layer carries a diagonal of its own, which the
-  // RZ(phi) factors join at no extra cost; alone, its two diagonals cost more
-  // than the real sweeps save
-  if (mats && !mats_dev && !active && n_terms > 0 && euler_enabled(h)) {
+  // RZ(phi) factors join at no extra cost; with RY sweeps in tangent form it
+  // pays for a bare U(2) layer as well (MQ_EULER_PLAIN)
+  if (mats && !mats_dev && !active && (n_terms > 0 || euler_plain()) && euler_enabled(h)) {
     // validate the layer's own terms before anything is launched
     if (n_terms > 0) {
       DiagWindows probe;
