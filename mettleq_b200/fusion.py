@@ -139,11 +139,19 @@ def dependency_schedule(ops: Sequence[dict]) -> List[dict]:
     succ: List[List[int]] = [[] for _ in range(count)]
     last: Dict[int, int] = {}
     for i, op in enumerate(ops):
-        preds = {last[w] for w in op.get("wires", []) if w in last}
+        wires = op.get("wires", ())
+        if len(wires) == 1:
+            p = last.get(wires[0])
+            if p is not None:
+                indeg[i] = 1
+                succ[p].append(i)
+            last[wires[0]] = i
+            continue
+        preds = {last[w] for w in wires if w in last}
         indeg[i] = len(preds)
         for p in preds:
             succ[p].append(i)
-        for w in op.get("wires", []):
+        for w in wires:
             last[w] = i
     cats = [_category(op) for op in ops]
     ready: Dict[str, list] = {}
