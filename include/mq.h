@@ -64,8 +64,9 @@ int mq_state_footprint(int n, int dtype, int double_buffered, uint64_t* out_byte
 
 /* ---- state handles (StateVectorSimulator, sim.py:17-45) ------------------ */
 /* stream: a cudaStream_t, or NULL for a stream owned by the handle.
- * Refuses n outside [1, 32] with MQ_EINVAL and allocation failure with
- * MQ_ENOMEM, before touching device memory. */
+ * Refuses n outside [1, 31] with MQ_EINVAL (the reference's limit,
+ * execution.py:23-25: 2^n amplitudes are counted in 32 bits) and
+ * allocation failure with MQ_ENOMEM, before touching device memory. */
 int mq_state_create(int n, int dtype, int device, void* stream, mq_state** out);
 int mq_state_destroy(mq_state* h);
 int mq_state_info(const mq_state* h, int* n, int* dtype, int* device);
@@ -211,7 +212,10 @@ int mq_batch_destroy(mq_batch* b);
  * GPU that loads it until the process exits; it holds the partial sums of
  * up to 1024 blocks, enough for GPUs of up to 256 SMs, and larger GPUs get
  * MQ_EUNSUPPORTED.  The first call on each device looks up the array's
- * device address; make that first call before any stream capture.  All
+ * device address; make that first call before any stream capture.  The
+ * address is kept for the life of the process: after a cudaDeviceReset of a
+ * device it is stale, so do not call this entry point on that device
+ * again.  All
  * calls on one device share the array: calls that overlap on the GPU (other
  * handles, other streams) race and must be serialised by the caller.  Each
  * call writes every scratch slot it reads, so nothing needs clearing

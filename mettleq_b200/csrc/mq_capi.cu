@@ -89,7 +89,7 @@ int mq_device_count(int* out) {
 
 int mq_state_footprint(int n, int dtype, int double_buffered, uint64_t* out_bytes) {
   if (!out_bytes) return fail(MQ_EINVAL, "null output");
-  if (n < 1 || n > kMaxQubits) return fail(MQ_EINVAL, "n_qubits must be in [1, 32]");
+  if (n < 1 || n > kMaxQubits) return fail(MQ_EINVAL, "n_qubits must be in [1, 31]");
   if (dtype != MQ_C64 && dtype != MQ_C128) return fail(MQ_EINVAL, "dtype must be MQ_C64 or MQ_C128");
   const uint64_t amp = dtype == MQ_C64 ? 8 : 16;
   const uint64_t state = (uint64_t(1) << n) * amp;
@@ -101,7 +101,7 @@ int mq_state_create(int n, int dtype, int device, void* stream, mq_state** out) 
   MQ_TRY_BEGIN
   if (!out) return fail(MQ_EINVAL, "null output handle");
   *out = nullptr;
-  if (n < 1 || n > kMaxQubits) return fail(MQ_EINVAL, "n_qubits must be in [1, 32]");
+  if (n < 1 || n > kMaxQubits) return fail(MQ_EINVAL, "n_qubits must be in [1, 31]");
   if (dtype != MQ_C64 && dtype != MQ_C128) return fail(MQ_EINVAL, "dtype must be MQ_C64 or MQ_C128");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {

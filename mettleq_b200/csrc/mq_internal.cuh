@@ -46,7 +46,10 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // ---------------------------------------------------------------- limits
-constexpr int kMaxQubits = 32;        // 32-bit amplitude indices
+// 31 qubits at most, the reference's limit (execution.py:23-25): the
+// amplitude count 2^n is carried in 32-bit variables (launch sizes, the
+// reductions' dimension), which cannot hold 2^32.
+constexpr int kMaxQubits = 31;
 constexpr int kTileMaxC64 = 13;       // 2^13 complex64 = 64 KiB tile
 constexpr int kTileMaxC128 = 12;      // 2^12 complex128 = 64 KiB tile
 

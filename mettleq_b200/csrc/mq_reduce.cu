@@ -484,7 +484,10 @@ int run_expval_pauli(mq_state* h, int n_words, const uint64_t* xmask, const uint
 // host reaches the array through the address that cudaGetSymbolAddress
 // returns for the current device (the array's name in host code is only a
 // host-side stand-in); the address is looked up once per device, on the
-// first call made on that device.
+// first call made on that device, and kept for the life of the process.  A
+// cudaDeviceReset (or any teardown of the device's primary context) makes
+// the kept address stale: a process that resets a device must not call this
+// entry point on it afterwards.
 constexpr uint32_t kStaticBlocks = 1024;  // partial-sum blocks the array holds
 static __device__ __align__(256) double2 g_pauli_static[kStaticBlocks * kWords + kWords];
 

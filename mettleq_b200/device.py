@@ -109,10 +109,12 @@ class Device:
         else:
             raise ValueError(f"Unknown fused layer: {name}")
 
-    # reference: device.py:541-554
-    def synchronize(self) -> StateVector:
+    # reference: device.py:541-554 (returns the simulator's state, which
+    # ``np.asarray(state, dtype=np.complex64)`` reads back like the MLX array
+    # the reference returns)
+    def synchronize(self):
         self.sim.synchronize()
-        return self.sim
+        return self.sim.state
 
     def statevector(self) -> np.ndarray:
         return self.sim.get()

@@ -77,6 +77,66 @@ def pauli_masks(n: int, word: Dict[int, str]) -> Tuple[int, int, int]:
     return x, z, ny
 
 
+class DeviceState:
+    """The ``state`` attribute of a ``StateVector``: a handle on the resident
+    device state, standing where the reference keeps its MLX array
+    (``StateVectorSimulator.state``, sim.py:32-45).
+
+    It supports exactly what the reference's SDK helpers do with that array
+    (integrations/_common.py:231-253): ``np.asarray(state, dtype)`` reads the
+    amplitudes back to the host, and ``sim.state = sim.state * factor``
+    multiplies the resident state by a complex scalar on the GPU (the
+    product is a deferred ``ScaledState`` that the setter applies), so
+    ``apply_global_phase`` never moves the state to the host."""
+
+    __array_priority__ = 1000  # numpy scalars on the left defer to __rmul__
+
+    def __init__(self, sv: "StateVector"):
+        self._sv = sv
+
+    @property
+    def shape(self) -> Tuple[int]:
+        return (1 << self._sv.n,)
+
+    @property
+    def dtype(self) -> np.dtype:
+        return self._sv.dtype
+
+    def __len__(self) -> int:
+        return 1 << self._sv.n
+
+    def __array__(self, dtype=None, copy=None):
+        out = self._sv.get()
+        return out if dtype is None else out.astype(dtype, copy=False)
+
+    def __mul__(self, factor) -> "ScaledState":
+        return ScaledState(self._sv, complex(factor))
+
+    __rmul__ = __mul__
+
+
+class ScaledState:
+    """``factor`` times a resident state, not yet applied: assigning it to
+    the same simulator's ``state`` multiplies the state on the GPU; reading
+    it with ``np.asarray`` gives the scaled amplitudes without changing the
+    resident state."""
+
+    __array_priority__ = 1000
+
+    def __init__(self, sv: "StateVector", factor: complex):
+        self._sv = sv
+        self.factor = complex(factor)
+
+    def __mul__(self, other) -> "ScaledState":
+        return ScaledState(self._sv, self.factor * complex(other))
+
+    __rmul__ = __mul__
+
+    def __array__(self, dtype=None, copy=None):
+        out = (self._sv.get() * self._sv.dtype.type(self.factor)).astype(self._sv.dtype)
+        return out if dtype is None else out.astype(dtype, copy=False)
+
+
 class StateVector:
     """One statevector resident in device memory (one CUDA stream)."""
 
@@ -136,6 +196,35 @@ class StateVector:
 
     def copy_from(self, other: "StateVector") -> None:
         N.check(self._lib.mq_state_copy(self._h, other._h))
+
+    # -- the reference simulator's state attribute (sim.py:32-45) -------------
+    @property
+    def state(self) -> DeviceState:
+        """The resident state (see ``DeviceState``)."""
+        return DeviceState(self)
+
+    @state.setter
+    def state(self, value) -> None:
+        if isinstance(value, ScaledState) and value._sv is self:
+            self.scale(value.factor)
+        elif isinstance(value, DeviceState) and value._sv is self:
+            return
+        elif isinstance(value, (DeviceState, ScaledState)):
+            if value._sv.n != self.n or value._sv.dtype != self.dtype:
+                raise ValueError("state has the wrong length or dtype")
+            self.copy_from(value._sv)
+            if isinstance(value, ScaledState):
+                self.scale(value.factor)
+        else:
+            self.set(value)
+
+    def scale(self, factor: complex) -> None:
+        """Multiply the resident state by a complex scalar (one diagonal pass,
+        the same factor on both values of qubit 0)."""
+        f = complex(factor)
+        if f == 1.0:
+            return
+        self.apply_diag_terms([(N.MQ_DIAG_1Q, 0, -1, [f.real, f.imag, f.real, f.imag])])
 
     @property
     def stream(self) -> int:
@@ -339,6 +428,42 @@ class StateVector:
         idx = self.sample_indices(shots, wires, seed=seed, stream_offset=stream_offset)
         shifts = np.arange(k - 1, -1, -1, dtype=np.int64)
         return ((idx[:, None] >> shifts) & 1).astype(np.int64)
+
+    # -- the reference simulator's measurement surface (sim.py:322-430) ------
+    def probabilities_array(self, wires: Optional[Sequence[int]] = None) -> np.ndarray:
+        """Full (None) or marginal probabilities in the requested wire order,
+        first wire = most significant bit, as float32 like the reference's
+        |amplitude|^2 of a complex64 state (sim.py:322-343); an empty list
+        gives [total probability].  Reduced on the GPU in float64."""
+        if wires is not None:
+            wires = [int(w) for w in wires]
+        return self.probabilities(wires, dtype=np.float32)
+
+    def sample_array(self, shots: int, wires: Optional[Sequence[int]] = None, *, rng=None) -> np.ndarray:
+        """``shots`` samples of ``wires`` (None = all) as int64 bit rows, first
+        wire = most significant (sim.py:383-419).  Draws one uint32 from
+        ``rng`` (``np.random.default_rng()`` when None) exactly as the
+        reference does (sim.py:405-408) and uses it as the key of the
+        engine's Philox4x32-10 stream, so one generator state fixes the
+        shots."""
+        shots = int(shots)
+        if shots < 0:
+            raise ValueError("shots must be non-negative")
+        rng = np.random.default_rng() if rng is None else rng
+        seed = int(rng.integers(0, np.iinfo(np.uint32).max, dtype=np.uint32))
+        return self.sample_bits(shots, None if wires is None else [int(w) for w in wires], seed=seed)
+
+    def sample(self, shots: int, wires: Optional[Sequence[int]] = None, *, rng=None) -> List[List[int]]:
+        """sim.py:421-422."""
+        return self.sample_array(shots, wires, rng=rng).tolist()
+
+    def sample_counts(self, shots: int, wires: Optional[Sequence[int]] = None, *, rng=None) -> Dict[str, int]:
+        """Bit-string counts, first wire leftmost (sim.py:424-430)."""
+        counts: Dict[str, int] = {}
+        for bits in self.sample_array(shots, wires, rng=rng):
+            key = "".join(str(int(b)) for b in bits)
+            counts[key] = counts.get(key, 0) + 1
+        return counts
 
     def expval_pauli(self, words: Sequence[Dict[int, str]]) -> np.ndarray:
         """<psi|P|psi> per Pauli word (pauli_product_expectations,

@@ -20,7 +20,9 @@ from . import fusion
 from ._native import StatevectorMemoryError
 
 STATEVECTOR_UNSAFE_OVERRIDE_ENV = "METTLEQ_ALLOW_UNSAFE_STATEVECTOR"
-INDEX_QUBIT_LIMIT = 32
+# 2^n amplitudes are counted in 32 bits, so 31 qubits at most (the
+# reference's METAL_INDEX_QUBIT_LIMIT, execution.py:23-25)
+INDEX_QUBIT_LIMIT = 31
 _TRUE = {"1", "true", "on", "yes", "enabled"}
 _FALSE = {"0", "false", "off", "no", "disabled", ""}
 

@@ -199,6 +199,8 @@ class Server:
         self._ladders: Dict[int, Tuple[List[int], int]] = {}
         self.peak_used = 0      # most footprint bytes admitted at once
         self.peak_active = 0    # most requests on the device at once
+        self.peak_large = 0     # most large requests on the device at once
+        self.partial_issues = 0  # issues of a chunk shorter than the request's remaining work
 
     def _ladder(self, n: int):
         if n not in self._ladders:
@@ -255,6 +257,7 @@ class Server:
                     # requests start without waiting for a whole-GPU sweep
                     sv.set_sm_limit(self._sms - self.sm_reserve if large else 0)
                     n_large += 1 if large else 0
+                    self.peak_large = max(self.peak_large, n_large)
                     r.admitted = now()
                     active.append({"req": r, "sv": sv, "stream": stream, "next": 0, "events": deque(),
                                    "large": large})
@@ -285,6 +288,8 @@ class Server:
                 left = len(r.layers) - a["next"]
                 chunk = left if (left << r.n) <= self.small_work else self.k
                 stop = min(len(r.layers), a["next"] + chunk)
+                if stop < len(r.layers):
+                    self.partial_issues += 1
                 for j in range(a["next"], stop):
                     apply_request_layer(a["sv"], r.layers[j], self._ladder(r.n))
                 a["next"] = stop

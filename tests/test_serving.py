@@ -73,6 +73,47 @@ def test_each_result_is_the_same_alone_and_in_the_mix():
         srv.close()
 
 
+def _mixed_with_large(seed):
+    """Ten small requests (6-14 qubits) and three large ones (22-24 qubits,
+    QFT and GF(2) layers likely) in one stream."""
+    from mettleq_b200.serving import random_layer
+    rng = np.random.default_rng(seed)
+    reqs = _small_requests(10, seed)
+    for j, n in enumerate((22, 23, 24)):
+        layers = [random_layer(n, rng, p_qft=0.5, p_xor=0.5) for _ in range(3)]
+        reqs.append(Request(10 + j, 0.0002 * j, n, layers, shots=1000, seed=77 + j))
+    return reqs
+
+
+@pytest.mark.gpu
+def test_large_requests_are_the_same_alone_and_in_the_mix():
+    """The branches the 30-qubit serving numbers depend on: large requests
+    (work above ``small_work``) run with an SM limit, at most ``max_large``
+    of them at once, and get their layers in chunks over several rounds.
+    Each result is bit-identical to the same request served alone; the
+    22-qubit one (and every small one) is within 1e-5 of the oracle."""
+    from mettleq_b200.serving import Server
+    mix = _mixed_with_large(5)
+    kw = dict(max_active=16, layers_per_round=1, keep_states=True, small_work=1 << 20, max_large=2,
+              sm_reserve=20)
+    srv = Server(**kw)
+    try:
+        stats = srv.serve(mix, realtime=False)
+        assert stats["requests"] == len(mix)
+        assert srv.peak_large == 2            # the cap engaged: three large requests, two at a time
+        assert srv.partial_issues > 0         # large requests were issued in chunks
+        assert srv.peak_active > 2
+        for r in mix:
+            alone = _mixed_with_large(5)[r.rid]
+            srv.serve([alone], realtime=False)
+            assert np.array_equal(alone.state, r.state), r.rid
+            assert np.array_equal(alone.samples, r.samples), r.rid
+            if r.n <= 22:
+                assert np.max(np.abs(r.state - _oracle_state(r))) < 1e-5, r.rid
+    finally:
+        srv.close()
+
+
 @pytest.mark.gpu
 def test_admission_stays_within_the_budget():
     from mettleq_b200.serving import Server

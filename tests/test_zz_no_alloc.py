@@ -75,6 +75,45 @@ def test_static_scratch_matches_allocating_entry_point(dtype, code):
         lib.mq_state_destroy(h)
 
 
+def test_static_scratch_long_mask_runs_and_optional_arguments():
+    """More than eight consecutive words on one X/Y mask (a pass holds eight,
+    so the run splits), runs of one mask broken up by other masks (the
+    allocating call groups them across the gap, this one does not), ny = NULL
+    and an empty word list: every value equals mq_expval_pauli's."""
+    from mettleq_b200 import _native as N
+    lib = N.lib()
+    n = 12
+    h = C.c_void_p()
+    assert lib.mq_state_create(n, 0, 0, None, C.byref(h)) == N.MQ_OK, N.last_error()
+    p = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    try:
+        vec = rand_state(n, 11, np.complex64)
+        assert lib.mq_state_set(h, p(vec)) == N.MQ_OK
+        # 11 words on X(1) in a row, then X(1) runs interleaved with X(4) words
+        words = [{1: "X", q: "Z"} for q in range(2, 12)] + [{1: "X"}]
+        for q in range(2, 8):
+            words += [{1: "X", q: "Z"}, {4: "X", q: "Z"}, {4: "X"}]
+        words += [{1: "Y", 3: "Z"}, {1: "Y"}]
+        got = _call(lib, "mq_expval_pauli_static", h, words, n)
+        ref = _call(lib, "mq_expval_pauli", h, words, n)
+        assert np.array_equal(got, ref), np.max(np.abs(got - ref))
+        # ny = NULL: no Y factors, results as with ny = 0
+        zw = [{q: "Z"} for q in range(n)] + [{2: "X", 5: "X"}] * 10
+        xs, zs, _ = _masks(n, zw)
+        a = np.full(2 * len(zw), np.nan)
+        b = np.full(2 * len(zw), np.nan)
+        assert lib.mq_expval_pauli_static(h, len(zw), p(xs), p(zs), None, p(a)) == N.MQ_OK, N.last_error()
+        assert lib.mq_expval_pauli(h, len(zw), p(xs), p(zs), None, p(b)) == N.MQ_OK, N.last_error()
+        assert np.array_equal(a, b)
+        # no words: nothing launched, nothing written
+        out = np.full(2, 7.0)
+        one = np.zeros(1, dtype=np.uint64)
+        assert lib.mq_expval_pauli_static(h, 0, p(one), p(one), None, p(out)) == N.MQ_OK, N.last_error()
+        assert np.array_equal(out, [7.0, 7.0])
+    finally:
+        lib.mq_state_destroy(h)
+
+
 def test_static_scratch_rejects_masks_outside_the_register():
     from mettleq_b200 import _native as N
     lib = N.lib()
