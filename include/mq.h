@@ -144,6 +144,11 @@ int mq_apply_xor_affine(mq_state* h, const uint64_t* rows, uint64_t c);
 /* wires == NULL or k < 0: full register in natural order.  out_dtype 0 =
  * float32, 1 = float64; out has 2^k (or 2^n) entries, first wire = MSB. */
 int mq_probabilities(mq_state* h, const int32_t* wires, int k, int out_dtype, void* out);
+/* The full probability vector (natural order, 2^n entries of out_dtype) into
+ * DEVICE memory of the handle's device, asynchronously on its stream: a
+ * caller that keeps results on the GPU (batched or pipelined circuits) reads
+ * nothing back.  Same values as mq_probabilities with wires == NULL. */
+int mq_probabilities_device(mq_state* h, int out_dtype, void* out_dev);
 /* Seeded inverse-CDF sampling over the marginal of wires (NULL/k<0 = all):
  * out[s] = outcome index (first wire = MSB) for s in [0, shots).  Philox4x32-10
  * stream keyed by seed, counter = s + stream_offset. */

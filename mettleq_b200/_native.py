@@ -54,6 +54,7 @@ SIGNATURES = {
     "mq_apply_xor_affine": (_I, [_P, _P, _U64]),
     "mq_apply_layer": (_I, [_P, _P, _P, _I, _P, _P, _P, _P, _U64]),
     "mq_probabilities": (_I, [_P, _P, _I, _I, _P]),
+    "mq_probabilities_device": (_I, [_P, _I, _P]),
     "mq_sample": (_I, [_P, _P, _I, _U64, _U64, _I64, _P]),
     "mq_expval_pauli": (_I, [_P, _I, _P, _P, _P, _P]),
     "mq_expval_pauli_static": (_I, [_P, _I, _P, _P, _P, _P]),

@@ -438,6 +438,25 @@ int mq_probabilities(mq_state* h, const int32_t* wires, int k, int out_dtype, vo
   MQ_TRY_END
 }
 
+int mq_probabilities_device(mq_state* h, int out_dtype, void* out_dev) {
+  MQ_TRY_BEGIN
+  MQ_CHECK_HANDLE(h);
+  if (!out_dev) return fail(MQ_EINVAL, "null output");
+  if (out_dtype != 0 && out_dtype != 1) return fail(MQ_EINVAL, "out_dtype must be 0 (float32) or 1 (float64)");
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, out_dev) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(MQ_EINVAL, "output is not a device pointer");
+  }
+  if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged)
+    return fail(MQ_EINVAL, "output is not device memory");
+  if (attr.type == cudaMemoryTypeDevice && attr.device != h->device)
+    return fail(MQ_EINVAL, "output lives on another device than the state");
+  DeviceGuard g(h->device);
+  return run_probabilities_device(h, out_dtype, out_dev);
+  MQ_TRY_END
+}
+
 int mq_sample(mq_state* h, const int32_t* wires, int k, uint64_t seed, uint64_t stream_offset, int64_t shots,
               int64_t* out) {
   MQ_TRY_BEGIN

@@ -45,6 +45,71 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// ---------------------------------------------------------------- TMA + mbarriers
+// Tile copies by the tensor memory accelerator: one thread issues a whole
+// tile (cp.async.bulk.tensor, up to 5 dimensions) that completes on an
+// mbarrier in shared memory; stores go back the same way from shared memory.
+// No cluster multicast is used anywhere: every copy moves this GPU's own
+// memory into (or out of) the issuing CTA's shared memory.
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// Waits for the phase of parity `parity` of the mbarrier to complete, for at
+// most `limit_ns` nanoseconds of the global timer; false when it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63u) == 0 && global_ns() - t0 > limit_ns) return false;
+  }
+}
+// Load box `coords` of tensor map `map` (a kernel parameter) into shared
+// memory at `dst`, completing `bytes` of transactions on `bar`.
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const void* map, const int32_t (&c)[5], uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], "
+      "[%7];\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tma_store_5d(const void* map, const int32_t (&c)[5], uint32_t src) {
+  asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];\n" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(src)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// The bulk stores issued so far have finished reading shared memory.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+// ... and finished writing global memory.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+// Generic-proxy writes to shared memory become visible to the async proxy
+// (a TMA store that reads them, a TMA load that overwrites them).
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
 // ---------------------------------------------------------------- limits
 // 31 qubits at most, the reference's limit (execution.py:23-25): the
 // amplitude count 2^n is carried in 32-bit variables (launch sizes, the
@@ -199,6 +264,7 @@ int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_t
 int launch_affine_cols(mq_state* h, const uint32_t* cols, uint32_t c);
 // Reductions (mq_reduce.cu)
 int run_probabilities(mq_state* h, const int32_t* wires, int k, int out_dtype, void* out);
+int run_probabilities_device(mq_state* h, int out_dtype, void* out_dev);
 int run_sample(mq_state* h, const int32_t* wires, int k, uint64_t seed, uint64_t offset,
                int64_t shots, int64_t* out);
 int run_expval_pauli(mq_state* h, int n_words, const uint64_t* xmask, const uint64_t* zmask,

@@ -306,6 +306,24 @@ static int check_wires(int n, const int32_t* wires, int k) {
   return MQ_OK;
 }
 
+// |a|^2 of every amplitude, natural order, into out (device memory of the
+// handle's device), asynchronously on the handle's stream.
+int run_probabilities_device(mq_state* h, int out_dtype, void* out) {
+  const uint32_t dim = (uint32_t)h->dim();
+  const uint32_t grid = (uint32_t)std::min<uint64_t>((dim + 255) / 256, (uint64_t)h->num_sms * 16);
+  if (h->dtype == MQ_C64) {
+    if (out_dtype == 0) k_amp2_out<float, float><<<grid, 256, 0, h->stream>>>((const float2*)h->cur_buf(), (float*)out, dim);
+    else k_amp2_out<float, double><<<grid, 256, 0, h->stream>>>((const float2*)h->cur_buf(), (double*)out, dim);
+  } else {
+    if (out_dtype == 0) k_amp2_out<double, float><<<grid, 256, 0, h->stream>>>((const double2*)h->cur_buf(), (float*)out, dim);
+    else k_amp2_out<double, double><<<grid, 256, 0, h->stream>>>((const double2*)h->cur_buf(), (double*)out, dim);
+  }
+  MQ_LAUNCHED("k_amp2_out");
+  h->launches += 1;
+  h->sweeps += 1;
+  return MQ_OK;
+}
+
 int run_probabilities(mq_state* h, const int32_t* wires, int k, int out_dtype, void* out) {
   int rc = check_wires(h->n, wires, k);
   if (rc) return rc;

@@ -406,6 +406,14 @@ class StateVector:
                                            int(w.size), code, _ptr(out)))
         return out
 
+    def probabilities_to_device(self, out_ptr: int, dtype=np.float32) -> None:
+        """The full probability vector into device memory at ``out_ptr``
+        (2^n entries of float32 or float64), asynchronously on the stream."""
+        dt = np.dtype(dtype)
+        if dt not in (np.float32, np.float64):
+            raise ValueError("probabilities dtype must be float32 or float64")
+        N.check(self._lib.mq_probabilities_device(self._h, 0 if dt == np.float32 else 1, C.c_void_p(int(out_ptr))))
+
     def sample_indices(self, shots: int, wires: Optional[Sequence[int]] = None, *, seed: int = 0,
                        stream_offset: int = 0) -> np.ndarray:
         shots = int(shots)

@@ -331,13 +331,56 @@ class Server:
         self.pool.close()
 
 
+def device_work(requests: List[Request], device: int = 0, host_s_per_layer: float = 5e-4) -> List[float]:
+    """Device time of each request's layers run alone (seconds, CUDA events):
+    the GPU first spins for longer than the host needs to issue all of the
+    request's layers, so the events bracket back-to-back kernels only and
+    their sum is a lower bound on any schedule's busy time (shots excluded:
+    one read of the state).  Spins are bounded (torch's clock-cycle sleep);
+    a request whose issue outlasted its spin is measured again with twice
+    the spin."""
+    import torch
+    pool = StatePool(device)
+    ladders: Dict[int, Tuple[List[int], int]] = {}
+    rate = 2.0e9  # spin cycles per second: at or above the SM clock, so a spin lasts at least its time
+    out = []
+    try:
+        for r in requests:
+            ladder = ladders.setdefault(r.n, cnot_ladder_rows(r.n))
+            sv, stream = pool.get(r.n)
+            spin = host_s_per_layer * max(1, len(r.layers))
+            for _ in range(6):
+                sv.reset()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                with torch.cuda.stream(stream):
+                    torch.cuda._sleep(int(spin * rate))
+                    e0.record(stream)
+                    for L in r.layers:
+                        apply_request_layer(sv, L, ladder)
+                    late = e0.query()  # the spin ended before the last layer was issued
+                    e1.record(stream)
+                e1.synchronize()
+                if not late:
+                    break
+                spin *= 2.0
+            out.append(e0.elapsed_time(e1) / 1e3)
+            pool.put(r.n, (sv, stream))
+    finally:
+        pool.close()
+    return out
+
+
 def serve_plain(requests: List[Request], realtime: bool = True, device: int = 0,
-                clock: Callable[[], float] = time.perf_counter) -> Dict[str, float]:
+                clock: Callable[[], float] = time.perf_counter, cache: Optional[dict] = None) -> Dict[str, float]:
     """The reference's serving model: one request at a time in arrival order,
     each through the op-dict runtime (Device.execute, integrations/_common.py
-    :118-228) and a seeded sample, its device state created per request."""
+    :118-228) and a seeded sample.  Devices are cached per width like the
+    reference's ``execution_cache`` (_common.py:166-195): a width seen before
+    reuses its state, reset to |0...0>."""
     from .device import Device
     from .workloads import affine_gates, qft_ops, u3_params
+    own = cache is None
+    cache = {} if own else cache
     t0 = clock()
     now = lambda: clock() - t0  # noqa: E731
     for r in sorted(requests, key=lambda x: x.arrival):
@@ -357,12 +400,18 @@ def serve_plain(requests: List[Request], realtime: bool = True, device: int = 0,
                 ops.extend(qft_ops(n))
             if L.xor is not None:
                 ops.extend(affine_gates(list(L.xor[0]), int(L.xor[1]), n))
-        dev = Device(n)
+        dev = cache.get(n)
+        if dev is None:
+            dev = cache[n] = Device(n, device_index=device)
+        else:
+            dev.reset()
         dev.execute(ops)
         r.samples = dev.sim.sample_indices(r.shots, seed=r.seed)
-        dev.close()
         r.finished = now()
     makespan = now()
+    if own:
+        for d in cache.values():
+            d.close()
     lat = np.array([r.latency for r in requests])
     return {"requests": len(requests), "makespan_s": makespan, "circuits_per_s": len(requests) / makespan,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),

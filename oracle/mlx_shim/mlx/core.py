@@ -1,10 +1,11 @@
 """numpy-backed stand-in for the subset of ``mlx.core`` the reference's CPU
 statevector path calls.
 
-Test infrastructure only: ``tests/golden/make_golden.py`` puts this package on
-``sys.path`` so that the reference's own ``Device(n, execution_device="cpu")``
-(device.py:73-431 -> sim.py per-gate routines) runs unchanged in a container
-without MLX, and records its outputs as golden vectors.  ``metal.is_available``
+Test and measurement infrastructure only: ``tests/golden/make_golden.py`` and
+``bench.py --impl reference`` put this package on ``sys.path`` so that the
+reference's own ``Device(n, execution_device="cpu")`` (device.py:73-431 ->
+sim.py per-gate routines) runs unchanged on a host without MLX, to record its
+outputs as golden vectors or to time it.  ``metal.is_available``
 answers False and ``fast.metal_kernel`` is absent, so the reference never
 selects its Metal shaders (execution.py:123-125, 156-183).
 

@@ -5,7 +5,7 @@ not read, anywhere else):
 
     python tests/golden/make_golden.py /path/to/MettleQ/src
 
-The reference imports ``mlx.core`` everywhere; ``tests/golden/mlx_shim``
+The reference imports ``mlx.core`` everywhere; ``oracle/mlx_shim``
 supplies a numpy-backed stand-in, with ``metal.is_available() == False`` so
 that ``Device(n, execution_device="cpu")`` takes its pure per-gate path
 (device.py:1138-1290, sim.py).  Outputs land in ``tests/golden/*.npz`` and
@@ -69,7 +69,7 @@ def _ops_layers(n: int, rng: np.random.Generator, layers: int, uniform_zz: bool)
 
 
 def main(src_root: str) -> None:
-    sys.path.insert(0, os.path.join(HERE, "mlx_shim"))
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "oracle", "mlx_shim"))
     sys.path.insert(0, src_root)
     import mlx.core as mx  # the shim
     from mettleq.device import Device
@@ -138,4 +138,6 @@ def main(src_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path to the MettleQ src directory>")
+    main(sys.argv[1])

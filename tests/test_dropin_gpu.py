@@ -319,10 +319,11 @@ def test_package_helpers_against_the_oracle():
             t = np.transpose(psi, wires + rest).reshape(4, -1)
             want = np.vdot(t, M @ t)
             assert abs(val - want) < 2e-5, wires
-        # Pauli words
+        # Pauli words (the complex64 state after ~130 gates keeps its norm to
+        # ~2e-6, so expectations are held to the amplitude bar, 1e-5)
         words = [{0: "Z"}, {1: "X", 4: "Y"}, {2: "Y", 3: "Y", 9: "Z"}, {}]
         vals = C.pauli_product_expectations(dev, words)
         for w, v in zip(words, vals):
-            assert abs(v - o.pauli_expectation(w)) < 2e-6, w
+            assert abs(v - o.pauli_expectation(w)) < 1e-5, w
     finally:
         dev.close()
