@@ -604,8 +604,10 @@ def run_reference(args):
     layer_bytes = 2 * (1 << n) * 8
     n_cpu = min(args.cpu_qubits, n)
     threads = cpu_threads()
+    # warm-up: builds the chunk devices and runs every gate once; the timed
+    # steps reuse them
     for _ in range(max(0, min(args.warmup, 1))):
-        cpu_baseline_sample(n, min(n_cpu, 20), circuit, threads=threads)  # code paths and allocator warm
+        cpu_baseline_sample(n, n_cpu, circuit, threads=threads)
     times, walls = [], []
     used, kind, sample = 1, "port", ""
     for _ in range(max(1, args.steps)):

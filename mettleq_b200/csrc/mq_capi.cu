@@ -120,6 +120,7 @@ int mq_state_create(int n, int dtype, int device, void* stream, mq_state** out) 
                   n, bytes / 1073741824.0, free_b / 1073741824.0);
     return fail(MQ_ENOMEM, msg);
   }
+  prepare_tile_maps();
   auto* h = new mq_state();
   h->n = n;
   h->dtype = dtype;
@@ -228,7 +229,7 @@ int mq_state_get(mq_state* h, void* host_amps) {
   DeviceGuard g(h->device);
   MQ_CUDA(cudaMemcpyAsync(host_amps, h->cur_buf(), h->state_bytes, cudaMemcpyDeviceToHost, h->stream));
   MQ_CUDA(cudaStreamSynchronize(h->stream));
-  return MQ_OK;
+  return check_tile_fault(h);
 }
 
 int mq_state_copy(mq_state* dst, const mq_state* src) {
@@ -252,7 +253,7 @@ int mq_sync(mq_state* h) {
   MQ_CHECK_HANDLE(h);
   DeviceGuard g(h->device);
   MQ_CUDA(cudaStreamSynchronize(h->stream));
-  return MQ_OK;
+  return check_tile_fault(h);
 }
 
 int mq_state_counters(const mq_state* h, uint64_t* launches, uint64_t* sweeps) {

@@ -218,6 +218,13 @@ struct DeviceGuard {
 
 int ensure_scratch(mq_state* h, size_t bytes);
 int ensure_alt(mq_state* h);  // allocate the second buffer if absent
+// After a synchronisation: MQ_ETIMEOUT (and the flag cleared) when a tile
+// sweep on the handle's device abandoned its work because a tile load did not
+// arrive in time, else MQ_OK (mq_tile.cu).
+int check_tile_fault(mq_state* h);
+// Looks up the driver's tensor-map encoder once per process (state creation
+// calls it, so that no lookup happens inside a stream capture).
+void prepare_tile_maps();
 
 // ------------------------------------------------------------ launchers
 // Tile sweeps: U(2) layer and QFT (mq_tile.cu)

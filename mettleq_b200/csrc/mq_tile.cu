@@ -38,6 +38,9 @@
 #include <mutex>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "mq_internal.cuh"
 
 namespace mq {
@@ -82,7 +85,35 @@ struct __align__(16) PhaseDesc {
 static_assert(offsetof(PhaseDesc, uf) % 16 == 0, "matrix rows must be 16-byte aligned");
 static_assert(sizeof(PhaseDesc) % 16 == 0, "PhaseDesc array stride must keep rows aligned");
 
+// TMA form of a sweep's tile movement.  The state is viewed as a tensor of
+// 8-byte words (complex64: one amplitude; complex128: its real or imaginary
+// part, word bit 0) whose dimensions are runs of index bits in ascending
+// order: dimension 0 is word bits [0, 4) (128 bytes), then alternately runs
+// of tile bits (box = the whole run, split at 8 bits) and runs of free bits
+// (box 1; coordinate = the tile base's bits there).  A tile is then one box,
+// and the tensor map's 128-byte swizzle puts 16-byte chunk j of 128-byte
+// row r at chunk j ^ (r & 7): the chunk layout the register phases already
+// use (amp_slot), so the phases read TMA-loaded tiles unchanged.
+struct alignas(64) TmaDesc {
+  CUtensorMap src;     // over the buffer the sweep reads
+  CUtensorMap dst;     // over the buffer it writes (the same one in place)
+  uint32_t bytes;      // one tile: the transaction count of one load
+  uint8_t ndim;        // 5 when the sweep runs in TMA form, else 0
+  uint8_t store;       // plain write-backs go out as TMA stores
+  uint8_t start[5];    // free dimension: first index bit of its run
+  uint32_t mask[5];    // free dimension: 2^len - 1 (0: a tile dimension)
+  // host side: the maps' shape (words of 8 bytes), encoded at launch
+  cuuint64_t gdim[5];
+  cuuint64_t gstride[4];
+  cuuint32_t box[5];
+};
+// a tile load that has not arrived after this long abandons the sweep
+constexpr uint64_t kTmaWaitNs = 2000000000ull;
+// set when a sweep was abandoned (read and cleared by mq_sync)
+__device__ unsigned int g_tile_fault;
+
 struct TileParams {
+  TmaDesc tma;
   uint32_t n_tiles;
   uint8_t n, m, n_phases, n_ops;
   uint8_t tile_bit[16];
@@ -463,7 +494,13 @@ __device__ __forceinline__ void apply_regdiag(V2<R> (&a)[16], const V2<R>* lut, 
 // phases plus the fused-layer epilogue (PT = FusedParams; a permuted or
 // window-diagonal write-back needs the tile bits [0, M)); MODE 3: U(2) phases
 // with register-phase diagonals only and the plain write-back.
-template <typename R, int M, int LR, int LT, int MODE, typename PT>
+//
+// TMA: tiles arrive by one tensor-map load per tile (P.tma), issued by
+// thread 0 and completed on an mbarrier per tile buffer; the plain write-back
+// leaves as one tensor-map store.  Every wait for a tile is bounded
+// (kTmaWaitNs); a CTA whose tile does not arrive in time records the fault
+// in g_tile_fault and returns as a whole.
+template <typename R, int M, int LR, int LT, int MODE, typename PT, bool TMA>
 __global__ void __launch_bounds__(1 << LT, (LT >= 9 ? 1 : (LT >= 8 ? (MODE == 2 ? MQ_MODE2_CTAS : 3) : (LT >= 7 ? (sizeof(R) == 4 && LR == 4 ? 6 : 3) : (LT >= 6 && sizeof(R) == 4 ? 8 : 1)))))
 k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   using T = V2<R>;
@@ -481,16 +518,31 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   constexpr int NBUF = tile_nbuf(M, LT);
   static_assert(GPT >= 1 && CPT >= 1, "bad tile configuration");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* bufs = reinterpret_cast<T*>(smem_raw);
-  PhaseDesc* phs = reinterpret_cast<PhaseDesc*>(smem_raw + NBUF * sizeof(T) * E);
+  // TMA tiles start on a 1024-byte boundary (the 128-byte swizzle repeats
+  // every 8 rows of 128 bytes, counted from the address), followed by one
+  // 8-byte mbarrier per tile buffer in a 64-byte slot; the host adds the
+  // slack for both
+  unsigned char* smem = smem_raw;
+  if constexpr (TMA) smem += (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
+  T* bufs = reinterpret_cast<T*>(smem);
+  constexpr size_t kBarBytes = TMA ? 64 : 0;
+  const uint32_t bar0 = smem_u32(smem + NBUF * sizeof(T) * E);
+  PhaseDesc* phs = reinterpret_cast<PhaseDesc*>(smem + NBUF * sizeof(T) * E + kBarBytes);
   const float2* tw = nullptr;
-  // shared memory: tile buffers, the launch's phase descriptors, then (MODE
-  // >= 2) the permutation columns and the diagonal tables
-  const size_t ph_end = NBUF * sizeof(T) * E + sizeof(PhaseDesc) * P.n_phases;
-  uint32_t* ecols = reinterpret_cast<uint32_t*>(smem_raw + ph_end);
-  T* qreg = reinterpret_cast<T*>(smem_raw + ph_end);  // MODE 1: per op, the register factors treg[32]
-  T* elut = reinterpret_cast<T*>(smem_raw + ph_end + 128);
+  // shared memory: tile buffers, (TMA) the mbarriers, the launch's phase
+  // descriptors, then (MODE >= 2) the permutation columns and the diagonal
+  // tables
+  const size_t ph_end = NBUF * sizeof(T) * E + kBarBytes + sizeof(PhaseDesc) * P.n_phases;
+  uint32_t* ecols = reinterpret_cast<uint32_t*>(smem + ph_end);
+  T* qreg = reinterpret_cast<T*>(smem + ph_end);  // MODE 1: per op, the register factors treg[32]
+  T* elut = reinterpret_cast<T*>(smem + ph_end + 128);
   const int tid = threadIdx.x;
+  if constexpr (TMA) {
+    if (tid == 0) {
+      for (int b = 0; b < NBUF; ++b) mbar_init(bar0 + 8u * b, 1);
+      mbar_init_fence();
+    }
+  }
   {
     const uint32_t words = (uint32_t)(sizeof(PhaseDesc) * P.n_phases / 4);
     const uint32_t* srcw = reinterpret_cast<const uint32_t*>(&P.ph[0]);
@@ -597,7 +649,24 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
 #pragma unroll
     for (int k = 0; k < CPT; ++k) cp_async<16>(sb + 16u * slot(k), src + (gb | g_k(k)));
   };
-  if constexpr (NBUF == 2) {
+  // TMA: the box coordinates of the tile whose base index is `base` (free
+  // dimensions take base's bits of their run, tile dimensions 0)
+  auto tma_coords = [&](uint32_t base, int32_t (&c)[5]) {
+#pragma unroll
+    for (int d = 0; d < 5; ++d) c[d] = (int32_t)((base >> P.tma.start[d]) & P.tma.mask[d]);
+  };
+  // TMA (thread 0): tile t into buffer b
+  auto tma_load_tile = [&](uint32_t t, int b) {
+    uint32_t cl;
+    int32_t c[5];
+    tma_coords(src_base(t, cl), c);
+    const uint32_t bar = bar0 + 8u * (uint32_t)b;
+    mbar_expect_tx(bar, P.tma.bytes);
+    tma_load_5d(smem_u32(bufs + b * E), &P.tma.src, c, bar);
+  };
+  if constexpr (TMA) {
+    if (tid == 0 && tile < P.n_tiles) tma_load_tile(tile, 0);
+  } else if constexpr (NBUF == 2) {
     if (tile < P.n_tiles) load_tile(tile, bufs);
     cp_async_commit();
   }
@@ -608,8 +677,23 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   constexpr bool LATE = NBUF == 2 && MQ_LATE_PREFETCH;
   T a[NR];
   for (int it = 0; tile < P.n_tiles; tile += gridDim.x, ++it) {
-    T* cur = bufs + (NBUF == 2 ? (it & 1) * E : 0);
-    if constexpr (LATE) {
+    const int cb = NBUF == 2 ? (it & 1) : 0;
+    T* cur = bufs + cb * E;
+    if constexpr (TMA) {
+      // every thread waits for the tile itself (acquiring the TMA's writes);
+      // if any wait gives up, the whole CTA records it and returns together
+      const uint32_t bar = bar0 + 8u * (uint32_t)cb;
+      const uint32_t parity = (uint32_t)((NBUF == 2 ? (it >> 1) : it) & 1);
+      const bool ok = mbar_wait_bounded(bar, parity, kTmaWaitNs);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicOr(&g_tile_fault, 1u);
+          mbar_wait_bounded(bar, parity, kTmaWaitNs);  // the load in flight, once more
+          bulk_wait_all();
+        }
+        return;
+      }
+    } else if constexpr (LATE) {
       cp_async_wait<0>();
       __syncthreads();
       const uint32_t next = tile + gridDim.x;
@@ -719,6 +803,17 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
             for (int r = 0; r < NR; ++r) a[r] = cmul(a[r], cmul(f, tr[r]));
           }
         }
+        if constexpr (QFT && TMA) {
+          // a TMA store writes the tile as it stands: the sweep's 2^{-stages/2}
+          // is applied here instead of in the write-back (the same product)
+          if (ph == P.n_phases - 1) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+              a[r].x *= (R)P.scale;
+              a[r].y *= (R)P.scale;
+            }
+          }
+        }
         if (pair) {
 #pragma unroll
           for (int r = 0; r < NR; r += 2)
@@ -729,12 +824,54 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
           for (int r = 0; r < NR; ++r) cur[sq ^ osel<LR>(r, sreg)] = a[r];
         }
       }
+      // TMA: the tile's last shared-memory writes become visible to the
+      // async proxy (the TMA store that reads them, the TMA load that will
+      // overwrite them) before the barrier
+      if constexpr (TMA)
+        if (ph == P.n_phases - 1) fence_proxy_async_smem();
       __syncthreads();
+      if constexpr (TMA && NBUF == 2) {
+        // after the first barrier of this tile every thread has finished the
+        // previous tile, so its buffer takes this CTA's next tile (once a TMA
+        // store from it has read it out)
+        if (ph == 0 && tid == 0) {
+          const uint32_t next = tile + gridDim.x;
+          if (next < P.n_tiles) {
+            if (P.tma.store) bulk_wait_read();
+            tma_load_tile(next, cb ^ 1);
+          }
+        }
+      }
     }
     if constexpr (STORE_EPI) {
       if (P.epi.perm || P.epi.diag) {
         epilogue_store<R, M, LT, CPT>(P.epi, cur, ecols, elut, dst, tile << M, base, cl_in, tid, epi_ak);
-        if constexpr (!LATE) __syncthreads();
+        if constexpr (TMA && NBUF == 1) {
+          __syncthreads();
+          const uint32_t next = tile + gridDim.x;
+          if (tid == 0 && next < P.n_tiles) tma_load_tile(next, 0);
+        } else if constexpr (!LATE && !TMA) {
+          __syncthreads();
+        }
+        continue;
+      }
+    }
+    if constexpr (TMA) {
+      if (P.tma.store) {
+        // in place: the tile goes back where it came from
+        if (tid == 0) {
+          int32_t c[5];
+          tma_coords(base, c);
+          tma_store_5d(&P.tma.dst, c, smem_u32(cur));
+          bulk_commit();
+          if constexpr (NBUF == 1) {
+            const uint32_t next = tile + gridDim.x;
+            if (next < P.n_tiles) {
+              bulk_wait_read();
+              tma_load_tile(next, 0);
+            }
+          }
+        }
         continue;
       }
     }
@@ -755,9 +892,19 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
       }
       *reinterpret_cast<float4*>(dst + (gb | g_k(k))) = v;
     }
-    if constexpr (!LATE) __syncthreads();
+    if constexpr (TMA && NBUF == 1) {
+      __syncthreads();
+      const uint32_t next = tile + gridDim.x;
+      if (tid == 0 && next < P.n_tiles) tma_load_tile(next, 0);
+    } else if constexpr (!LATE && !TMA) {
+      __syncthreads();
+    }
   }
-  cp_async_wait<0>();
+  if constexpr (TMA) {
+    if (tid == 0) bulk_wait_all();  // the last TMA stores have written global memory
+  } else {
+    cp_async_wait<0>();
+  }
 }
 
 // ---------------------------------------------------------------- host side
@@ -858,11 +1005,49 @@ static void make_phases(int m, int lr, const std::vector<int>& order, Sweep& sw,
   }
 }
 
-template <typename R, int M, int LR, int LT, int MODE, typename PT>
-static int launch_tile_t(mq_state* h, const PT& P, size_t smem, bool out_of_place) {
-  auto kern = k_tile<R, M, LR, LT, MODE, PT>;
+// cuTensorMapEncodeTiled from the driver, looked up once (the runtime hands
+// out driver entry points, so the library needs no link against libcuda)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+void prepare_tile_maps() { (void)tensor_map_encoder(); }
+
+// The tensor maps of a TMA sweep over the buffers it reads and writes.
+static int encode_tile_maps(TmaDesc& D, void* src, void* dst) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return fail(MQ_EDEVICE, "cuTensorMapEncodeTiled is not available from the CUDA driver");
+  const cuuint32_t estride[5] = {1, 1, 1, 1, 1};
+  for (int k = 0; k < 2; ++k) {
+    const CUresult r = enc(k ? &D.dst : &D.src, CU_TENSOR_MAP_DATA_TYPE_UINT64, 5, k ? dst : src, D.gdim, D.gstride,
+                           D.box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(MQ_EDEVICE, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+  }
+  return MQ_OK;
+}
+
+template <typename R, int M, int LR, int LT, int MODE, typename PT, bool TMA>
+static int launch_tile_t(mq_state* h, PT& P, size_t smem, bool out_of_place) {
+  auto kern = k_tile<R, M, LR, LT, MODE, PT, TMA>;
   // the caller sized shared memory for two tile buffers
   if (tile_nbuf(M, LT) == 1) smem -= sizeof(V2<R>) << M;
+  if constexpr (TMA) {
+    smem += 1024 + 64;  // 1024-byte alignment of the tiles, the mbarriers
+    int rc = encode_tile_maps(P.tma, h->buf[h->cur], out_of_place ? h->buf[1 - h->cur] : h->buf[h->cur]);
+    if (rc) return rc;
+  }
   // the opt-in shared-memory limit only grows; resident CTAs per SM depend on
   // this launch's shared memory (rounded up to 1 KiB), looked up per size
   static std::mutex mu;
@@ -896,14 +1081,25 @@ static int launch_tile_t(mq_state* h, const PT& P, size_t smem, bool out_of_plac
   return MQ_OK;
 }
 
+// TMA form for the tiles of 10 bits and more (the sweeps of large states);
+// smaller tiles, and sweeps whose tile the TMA form cannot describe, keep the
+// per-thread asynchronous copies.
+template <typename R, int M, int LR, int LT, int MODE, typename PT>
+static int launch_tile_sel(mq_state* h, PT& P, size_t smem, bool oop) {
+  if constexpr (M >= 10 && LR == 4 && LT <= 8) {
+    if (P.tma.ndim) return launch_tile_t<R, M, LR, LT, MODE, PT, true>(h, P, smem, oop);
+  }
+  return launch_tile_t<R, M, LR, LT, MODE, PT, false>(h, P, smem, oop);
+}
+
 template <typename R, int MODE, int LR, typename PT>
-static int dispatch_tile_lr(mq_state* h, const PT& P, size_t smem, bool oop) {
+static int dispatch_tile_lr(mq_state* h, PT& P, size_t smem, bool oop) {
   switch (P.m) {
 #define MQ_TILE_CASE(MM)                                                        \
     case MM: {                                                                  \
       constexpr int L = (MM) < LR ? (MM) : LR;                                  \
       constexpr int LT = ((MM) - L) < 8 ? ((MM) - L) : 8;                       \
-      return launch_tile_t<R, MM, L, LT, MODE, PT>(h, P, smem, oop);            \
+      return launch_tile_sel<R, MM, L, LT, MODE, PT>(h, P, smem, oop);          \
     }
     MQ_TILE_CASE(1) MQ_TILE_CASE(2) MQ_TILE_CASE(3) MQ_TILE_CASE(4) MQ_TILE_CASE(5) MQ_TILE_CASE(6)
     MQ_TILE_CASE(7) MQ_TILE_CASE(8) MQ_TILE_CASE(9) MQ_TILE_CASE(10) MQ_TILE_CASE(11)
@@ -911,13 +1107,13 @@ static int dispatch_tile_lr(mq_state* h, const PT& P, size_t smem, bool oop) {
     case 12:
       if constexpr (sizeof(R) == 4) {
         constexpr int LT = LR == 5 ? 7 : 8;
-        return launch_tile_t<R, 12, LR, LT, MODE, PT>(h, P, smem, oop);
+        return launch_tile_sel<R, 12, LR, LT, MODE, PT>(h, P, smem, oop);
       }
       break;
     case 13:
       if constexpr (sizeof(R) == 4 && LR == 4) {
-        if (tile13_lt() == 8) return launch_tile_t<R, 13, 4, 8, MODE, PT>(h, P, smem, oop);
-        return launch_tile_t<R, 13, 4, 9, MODE, PT>(h, P, smem, oop);
+        if (tile13_lt() == 8) return launch_tile_sel<R, 13, 4, 8, MODE, PT>(h, P, smem, oop);
+        return launch_tile_sel<R, 13, 4, 9, MODE, PT>(h, P, smem, oop);
       }
       break;
     default: break;
@@ -926,7 +1122,7 @@ static int dispatch_tile_lr(mq_state* h, const PT& P, size_t smem, bool oop) {
 }
 
 template <typename R, int MODE, typename PT>
-static int dispatch_tile(mq_state* h, const PT& P, size_t smem, bool oop) {
+static int dispatch_tile(mq_state* h, PT& P, size_t smem, bool oop) {
   if constexpr (MODE >= 2) {
     return dispatch_tile_lr<R, MODE, 4>(h, P, smem, oop);
   } else {
@@ -1057,6 +1253,70 @@ static void fill_epi(EpiDesc& D, const EpiPlan& e, int m, int n) {
   D.n_entries = off;
 }
 
+// Tile movement by TMA (MQ_TMA=0: per-thread asynchronous copies throughout).
+static bool tma_enabled() { return env_int("MQ_TMA", 1, 0, 1) == 1; }
+
+int check_tile_fault(mq_state* h) {
+  unsigned int v = 0;
+  MQ_CUDA(cudaMemcpyFromSymbolAsync(&v, g_tile_fault, sizeof(v), 0, cudaMemcpyDeviceToHost, h->stream));
+  MQ_CUDA(cudaStreamSynchronize(h->stream));
+  if (!v) return MQ_OK;
+  const unsigned int zero = 0;
+  MQ_CUDA(cudaMemcpyToSymbolAsync(g_tile_fault, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, h->stream));
+  MQ_CUDA(cudaStreamSynchronize(h->stream));
+  return fail(MQ_ETIMEOUT, "a tile sweep on this device abandoned its work: a tile load did not arrive within 2 s");
+}
+
+// The TMA shape of a sweep's tiles (see TmaDesc): false when it needs more
+// than five dimensions or the tile lacks the low 128 bytes of its rows.
+// Dimensions of size 1 above the state pad the maps to five.
+static bool plan_tma(int n, size_t amp_bytes, const std::vector<int>& tile_bits, TmaDesc& D) {
+  const int s = amp_bytes == 16 ? 1 : 0;  // word bits below the amplitude bits (real / imaginary part)
+  const int nw = n + s;
+  if (nw < 4) return false;
+  std::vector<bool> tb(nw, false);
+  for (int w = 0; w < s; ++w) tb[w] = true;
+  for (int b : tile_bits) tb[b + s] = true;
+  for (int w = 0; w < 4; ++w)
+    if (!tb[w]) return false;
+  int nd = 0;
+  auto add = [&](int w0, int len, bool tile) -> bool {
+    if (nd == 5) return false;
+    D.gdim[nd] = cuuint64_t(1) << len;
+    D.box[nd] = tile ? (cuuint32_t(1) << len) : 1u;
+    if (nd > 0) D.gstride[nd - 1] = cuuint64_t(8) << w0;
+    D.start[nd] = (uint8_t)(tile ? 0 : w0 - s);
+    D.mask[nd] = tile ? 0u : (uint32_t)((uint64_t(1) << len) - 1u);
+    ++nd;
+    return true;
+  };
+  add(0, 4, true);
+  for (int w = 4; w < nw;) {
+    const bool t = tb[w];
+    int e = w;
+    while (e < nw && tb[e] == t) ++e;
+    if (t) {
+      for (int a = w; a < e; a += 8)
+        if (!add(a, std::min(8, e - a), true)) return false;
+    } else if (!add(w, e - w, false)) {
+      return false;
+    }
+    w = e;
+  }
+  const cuuint64_t total = cuuint64_t(8) << nw;
+  while (nd < 5) {
+    D.gdim[nd] = 1;
+    D.box[nd] = 1;
+    D.gstride[nd - 1] = total;
+    D.start[nd] = 0;
+    D.mask[nd] = 0;
+    ++nd;
+  }
+  D.ndim = 5;
+  D.bytes = (uint32_t)(amp_bytes << tile_bits.size());
+  return true;
+}
+
 static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, const std::vector<int>& op_rk,
                      const EpiPlan* epi = nullptr) {
   const int m = (int)sw.tile_bits.size();
@@ -1079,6 +1339,11 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
   P.n_ops = (uint8_t)sw.ops.size();
   for (int k = 0; k < m; ++k) P.tile_bit[k] = (uint8_t)sw.tile_bits[k];
   make_base_runs(P.runs, h->n, P.tile_bit, m);
+  // TMA form for tiles of 10 bits and more whose shape it can describe;
+  // the write-back is a TMA store unless it scatters (permutation) or
+  // multiplies per amplitude (window diagonal)
+  if (tma_enabled() && m >= 10 && !sw.phases.empty() && plan_tma(h->n, h->amp_bytes(), sw.tile_bits, P.tma))
+    P.tma.store = (epi && (epi->perm || epi->diag)) ? 0 : 1;
   // chunk-index bits above the thread bits: contiguous global bits?
   {
     const int cb = h->dtype == MQ_C64 ? 1 : 0;
