@@ -44,9 +44,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["scale", "batch", "adjoint", "serve"], default="scale",
+    ap.add_argument("--workload", choices=["scale", "batch", "adjoint", "serve", "sharded"], default="scale",
                     help="scale (the headline line), batch (4096 mixed circuits in one graph), adjoint "
-                         "(24-qubit gradient of 384 parameters), serve (Poisson request stream)")
+                         "(24-qubit gradient of 384 parameters), serve (Poisson request stream), sharded "
+                         "(one state of qubits + log2 N qubits over the N GPUs)")
     ap.add_argument("--count", type=int, default=None, help="circuits (batch) or requests (serve)")
     ap.add_argument("--qubits", type=int, default=30)
     ap.add_argument("--layers", type=int, default=40)
@@ -410,7 +411,7 @@ def _timed_clocks(fn, index: int = 0):
     return r, clk
 
 
-def run_batch(args, count=None, steps=None, device: int = 0, indices=None):
+def run_batch(args, count=None, steps=None, device: int = 0, indices=None, plain: bool = True):
     """Hardware-efficient-ansatz circuits (n ~ U{10..24}, depth ~ U{4..16},
     RY/RZ angles U[-pi, pi], CNOT ladder), complex64, in one CUDA-graph launch
     per batch; beside it the plain path (one circuit at a time through
@@ -458,9 +459,9 @@ def run_batch(args, count=None, steps=None, device: int = 0, indices=None):
     t_run = statistics.median(ts)
     # plain path on a sample: Device.execute, the probability vector into
     # device memory, <Z_0> to the host
-    sample = list(range(0, mine, max(1, mine // 256)))
+    sample = list(range(0, mine, max(1, mine // 256))) if plain else []
     devs = {}
-    buf = torch.empty(1 << max(ns[i] for i in sample), dtype=torch.float32, device=f"cuda:{device}")
+    buf = torch.empty(1 << max([ns[i] for i in sample] + [1]), dtype=torch.float32, device=f"cuda:{device}")
     err = 0.0
     t0 = time.perf_counter()
     for i in sample:
@@ -479,7 +480,7 @@ def run_batch(args, count=None, steps=None, device: int = 0, indices=None):
         d.close()
     n_small, n_large = b.n_small, b.n_large
     b.close()
-    plain_cps = len(sample) / t_plain
+    plain_cps = len(sample) / t_plain if sample else None
     value = mine / t_run
     return {
         "metric": "batched circuits/s", "value": value, "unit": "circuits/s", "n_gpus": 1, "steps": steps,
@@ -495,7 +496,7 @@ def run_batch(args, count=None, steps=None, device: int = 0, indices=None):
         "plain": {"circuits_per_s": plain_cps, "sample": len(sample),
                   "path": "one circuit at a time: Device.execute(op dicts) + probabilities into device memory "
                           "+ <Z_0> to the host; Devices cached per width"},
-        "speedup_vs_plain": value / plain_cps, "z0_max_diff_vs_plain": err, "clocks": clk,
+        "speedup_vs_plain": value / plain_cps if plain_cps else None, "z0_max_diff_vs_plain": err, "clocks": clk,
     }
 
 
@@ -595,6 +596,117 @@ def compact(d: dict, keys) -> dict:
     return {k: d[k] for k in keys if k in d}
 
 
+def run_batch_ranks(args, rank, world, local_rank, dist):
+    """The batch over N GPUs: each rank runs its share (longest-processing-
+    time split by depth x 2^n) as its own captured graph; value = all
+    circuits over the slowest rank's median step."""
+    from mettleq_b200.batch import hea_batch
+    from mettleq_b200.replicas import gather_objects, max_over_ranks, partition_by_cost
+    count = args.count or 4096
+    ns, ds, _ = hea_batch(count, seed=args.seed)
+    mine = partition_by_cost([d << n for n, d in zip(ns, ds)], world)[rank]
+    dist.barrier()
+    r = run_batch(args, count=count, indices=mine, device=local_rank, plain=False)
+    t = max_over_ranks(r["ms_per_step"] / 1e3, dist, device=f"cuda:{local_rank}")
+    shares = gather_objects(len(mine), dist)
+    r.update({"value": count / t, "n_gpus": world, "ms_per_step": t * 1e3, "scaling": "strong",
+              "circuits_per_rank": shares, "parallelism": f"replicas x{world}"})
+    r["config"]["circuits"] = count
+    return r
+
+
+def run_serve_ranks(args, rank, world, local_rank, dist):
+    """The request stream over N GPUs at N x 200 requests/s (weak scaling):
+    one queue per GPU (``assign_by_work``: each arrival to the GPU with the
+    least work so far), a Server per rank, latencies gathered to rank 0."""
+    from mettleq_b200.replicas import gather_objects, max_over_ranks
+    from mettleq_b200.serving import Server, assign_by_work, poisson_requests
+    count = (args.count or 200) * world
+    reqs = poisson_requests(count, rate=200.0 * world, seed=args.seed)
+    mine = [reqs[i] for i in assign_by_work(reqs, world)[rank]]
+    srv = Server(budget_bytes=150 * 10 ** 9, device=local_rank)
+    srv.serve(poisson_requests(8, seed=99, n_range=(12, 16), depth_range=(2, 3)), realtime=False)
+    dist.barrier()
+    stats, clk = _timed_clocks(lambda: srv.serve(mine, realtime=True), local_rank)
+    srv.close()
+    makespan = max_over_ranks(stats["makespan_s"], dist, device=f"cuda:{local_rank}")
+    lat = np.concatenate([np.asarray(x) for x in gather_objects([r.latency for r in mine], dist)])
+    return {
+        "metric": "serve p50 latency", "value": float(np.percentile(lat, 50)), "unit": "s", "n_gpus": world,
+        "steps": 1, "warmup": 1, "ms_per_step": makespan * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded Poisson request stream)",
+        "config": {"workload": f"serve: {count} requests, Poisson {200 * world} req/s over {world} GPUs (one queue "
+                               "each), n log-uniform 12..30, depth U{10..100}, QFT/XOR p=0.1, 1000 shots, "
+                               "150 GB budget per GPU"},
+        "p99_s": float(np.percentile(lat, 99)), "circuits_per_s": count / makespan, "makespan_s": makespan,
+        "requests_per_rank": gather_objects(len(mine), dist), "clocks": clk,
+    }
+
+
+def run_sharded(args, rank, world, local_rank, dist):
+    """One state sharded over the N ranks: n = qubits-per-GPU + log2 N
+    (8 GiB of complex64 per GPU at 30), layers of the scale structure (Haar
+    U(2) on every qubit, RZZ chain, CNOT ladder); a layer touching global
+    qubits swaps them with local ones by one all-to-all, the ladder remaps
+    whole shards between ranks.  Time: CUDA events on each rank's shard
+    stream, max over ranks."""
+    import torch
+    from mettleq_b200 import workloads as W
+    from mettleq_b200.fusion import DIAG_ZZ
+    from mettleq_b200.replicas import gather_objects, max_over_ranks
+    from mettleq_b200.sharded import GpuShard, ShardedState
+    g = int(round(math.log2(world)))
+    n = args.qubits + g
+    layers = min(args.layers, 10)
+    circuit = W.plain_circuit(n, layers, seed=args.seed)
+    shard = GpuShard(n - g, "complex64", device=local_rank)
+    st = ShardedState(n, shard, dist if world > 1 else None)
+    ladder = W.cnot_ladder_rows(n)
+    terms = [[(DIAG_ZZ, i, i + 1, [float(t) / 2.0]) for i, t in enumerate(L.thetas)] for L in circuit.layers]
+
+    def step():
+        st.reset()
+        for L, tm in zip(circuit.layers, terms):
+            st.apply_layer(L.mats, None, tm, *ladder)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ex0, rm0, by0 = st.exchanges, st.remaps, st.bytes_sent
+    l0 = shard.sv.counters()[0]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    e0.record(shard.stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(shard.stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist is not None:
+        dist.barrier()
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, device=f"cuda:{local_rank}")
+    sent = gather_objects((st.bytes_sent - by0) / args.steps, dist)
+    launches = shard.sv.counters()[0] - l0
+    logical = 3 * layers
+    total_bytes = (1 << n) * 8
+    shard.close()
+    return {
+        "metric": "sharded layer GB/s", "value": args.steps * logical * 2 * total_bytes / t / 1e9, "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": t / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "data": "synthetic (seeded Haar U(2), RZZ angles)",
+        "config": {"workload": f"sharded: {n} qubits complex64 over {world} GPU(s) ({n - g} local qubits each), "
+                               f"{layers} layers of U(2)+RZZ chain+CNOT ladder",
+                   "qubits": n, "global_qubits": g, "layers": layers, "logical_layers_per_step": logical,
+                   "state_bytes": total_bytes, "parallelism": f"sharded x{world}"},
+        "exchanges_per_step": (st.exchanges - ex0) / args.steps, "remaps_per_step": (st.remaps - rm0) / args.steps,
+        "bytes_sent_per_rank_per_step": sent, "gpu_launches": launches, "clocks": clk,
+    }
+
+
 # ---------------------------------------------------------------- reference arm
 def run_reference(args):
     from mettleq_b200 import workloads as W
@@ -640,10 +752,16 @@ def main():
             return 0
         print(json.dumps(run_reference(args)), flush=True)
         return 0
-    if args.workload != "scale":
+    if world == 1 and args.workload in ("batch", "adjoint", "serve"):
+        fn = {"batch": run_batch, "adjoint": run_adjoint, "serve": run_serve}[args.workload]
+        print(json.dumps(fn(args)), flush=True)
+        return 0
+    if args.workload == "adjoint":
+        # one gradient job: rank 0 alone
         if rank == 0:
-            fn = {"batch": run_batch, "adjoint": run_adjoint, "serve": run_serve}[args.workload]
-            print(json.dumps(fn(args)), flush=True)
+            import torch
+            torch.cuda.set_device(local_rank)
+            print(json.dumps(run_adjoint(args)), flush=True)
         return 0
     dist = None
     if world > 1:
@@ -654,6 +772,12 @@ def main():
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = td
     try:
+        if args.workload != "scale":
+            fn = {"batch": run_batch_ranks, "serve": run_serve_ranks, "sharded": run_sharded}[args.workload]
+            out = fn(args, rank, world, local_rank, dist)
+            if rank == 0:
+                print(json.dumps(out), flush=True)
+            return 0
         out = run_ours(args, rank, world, local_rank, dist)
         if rank == 0 and world == 1 and not args.no_extras:
             # the metric's other two parts on the same GPU, bounded in size:

@@ -2,9 +2,11 @@
 
 A 30-qubit state fits one B200 and batched / served circuits are independent,
 so several GPUs run replicas: each rank (one process per GPU) takes its share
-of the units, and the only collective is the timing reduction (the slowest
-rank's device time defines the job's time).  Sharding one state across GPUs
-is not built.
+of the units (``partition_by_cost`` for a batch, ``serving.assign_by_work``
+for a request stream), and the only collectives are the timing reduction
+(the slowest rank's time defines the job's time) and the gathering of
+per-rank results.  One state larger than a GPU is sharded instead
+(``mettleq_b200.sharded``).
 """
 from __future__ import annotations
 
@@ -27,6 +29,16 @@ def partition_by_cost(costs: Sequence[float], world: int) -> List[List[int]]:
     for p in parts:
         p.sort()
     return parts
+
+
+def gather_objects(obj, dist=None) -> list:
+    """Every rank's ``obj`` in rank order, on every rank (a pickled
+    all-gather; for per-rank results such as latency lists and counters)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return [obj]
+    out = [None] * dist.get_world_size()
+    dist.all_gather_object(out, obj)
+    return out
 
 
 def max_over_ranks(seconds: float, dist=None, device: str = "cpu") -> float:

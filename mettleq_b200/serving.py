@@ -184,7 +184,10 @@ class Server:
     def __init__(self, budget_bytes: int = 150 * 10 ** 9, max_active: int = 64, layers_per_round: int = 4,
                  max_bypass_s: float = 30.0, device: int = 0, keep_states: bool = False,
                  round_budget_s: float = 0.004, small_work: int = 100 << 22, max_large: int = 8,
-                 sm_reserve: int = 20):
+                 sm_reserve: int = 20, devices: Optional[List[int]] = None):
+        # budget_bytes, max_large and sm_reserve hold per device; with several
+        # devices every request goes to the device with the least footprint
+        # admitted that has room for it (one queue per device)
         self.budget = int(budget_bytes)
         self.max_active = int(max_active)
         self.k = int(layers_per_round)
@@ -193,11 +196,14 @@ class Server:
         self.max_large = int(max_large)                # large requests on the device at once
         self.sm_reserve = int(sm_reserve)              # SMs large requests leave to the others
         self.max_bypass_s = float(max_bypass_s)
-        self.device = int(device)
+        self.devices = [int(d) for d in devices] if devices else [int(device)]
+        self.device = self.devices[0]
         self.keep_states = keep_states
-        self.pool = StatePool(self.device)
+        self.pools = {d: StatePool(d) for d in self.devices}
+        self.pool = self.pools[self.device]
+        self.served_on: Dict[int, int] = {d: 0 for d in self.devices}  # requests admitted per device
         self._ladders: Dict[int, Tuple[List[int], int]] = {}
-        self.peak_used = 0      # most footprint bytes admitted at once
+        self.peak_used = 0      # most footprint bytes admitted at once on one device
         self.peak_active = 0    # most requests on the device at once
         self.peak_large = 0     # most large requests on the device at once
         self.partial_issues = 0  # issues of a chunk shorter than the request's remaining work
@@ -214,7 +220,7 @@ class Server:
         admitted / finished / samples of each request and returns summary
         statistics (latency = finished - arrival)."""
         import torch
-        self._sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        sms = {d: torch.cuda.get_device_properties(d).multi_processor_count for d in self.devices}
         for r in requests:
             if r.footprint > self.budget:
                 raise MemoryError(f"request {r.rid}: {r.n} qubits need {r.footprint} bytes, budget {self.budget}")
@@ -223,7 +229,7 @@ class Server:
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         waiting: List[Request] = []
         active: List[dict] = []
-        used = 0
+        used = {d: 0 for d in self.devices}
         done = 0
         while done < len(requests):
             t = now()
@@ -238,31 +244,35 @@ class Server:
                 else:
                     waiting.sort(key=lambda r: r.work)
             i = 0
-            n_large = sum(1 for a in active if a["large"])
+            n_large = {d: sum(1 for a in active if a["large"] and a["dev"] == d) for d in self.devices}
             while i < len(waiting) and len(active) < self.max_active:
                 r = waiting[i]
                 large = r.work > self.small_work
-                if large and n_large >= self.max_large:
-                    i += 1
-                    continue
-                if used + r.footprint <= self.budget:
-                    reuse = bool(self.pool.free.get(r.n))
+                # the device with the least footprint admitted among those
+                # with room (and a free large-request slot when it is large)
+                fits = [d for d in self.devices if used[d] + r.footprint <= self.budget
+                        and not (large and n_large[d] >= self.max_large)]
+                if fits:
+                    dev = min(fits, key=lambda d: (used[d], d))
+                    pool = self.pools[dev]
+                    reuse = bool(pool.free.get(r.n))
                     if not reuse:
-                        over = used + r.footprint + self.pool.bytes_free - self.budget
+                        over = used[dev] + r.footprint + pool.bytes_free - self.budget
                         if over > 0:
-                            self.pool.evict(over)
-                    sv, stream = self.pool.get(r.n)
+                            pool.evict(over)
+                    sv, stream = pool.get(r.n)
                     sv.reset()
                     # large requests leave SMs free, so the kernels of short
                     # requests start without waiting for a whole-GPU sweep
-                    sv.set_sm_limit(self._sms - self.sm_reserve if large else 0)
-                    n_large += 1 if large else 0
-                    self.peak_large = max(self.peak_large, n_large)
+                    sv.set_sm_limit(sms[dev] - self.sm_reserve if large else 0)
+                    n_large[dev] += 1 if large else 0
+                    self.peak_large = max(self.peak_large, n_large[dev])
                     r.admitted = now()
                     active.append({"req": r, "sv": sv, "stream": stream, "next": 0, "events": deque(),
-                                   "large": large})
-                    used += r.footprint
-                    self.peak_used = max(self.peak_used, used)
+                                   "large": large, "dev": dev})
+                    used[dev] += r.footprint
+                    self.served_on[dev] += 1
+                    self.peak_used = max(self.peak_used, used[dev])
                     self.peak_active = max(self.peak_active, len(active))
                     waiting.pop(i)
                     continue
@@ -309,8 +319,8 @@ class Server:
                     if self.keep_states:
                         r.state = a["sv"].get()
                     r.finished = now()
-                    used -= r.footprint
-                    self.pool.put(r.n, (a["sv"], a["stream"]))
+                    used[a["dev"]] -= r.footprint
+                    self.pools[a["dev"]].put(r.n, (a["sv"], a["stream"]))
                     done += 1
                     progressed = True
                 else:
@@ -328,7 +338,26 @@ class Server:
                 "mean_s": float(lat.mean())}
 
     def close(self) -> None:
-        self.pool.close()
+        for p in self.pools.values():
+            p.close()
+
+
+def assign_by_work(requests: List[Request], n_devices: int) -> List[List[int]]:
+    """One queue per device for a request stream split over processes (one
+    per GPU): in arrival order, each request goes to the device with the
+    least work (layers x 2^n) assigned so far (ties to the lowest device).
+    Only earlier arrivals decide a request's device, so the rule can run
+    online, and every process computes the same split.  Returns request
+    positions per device."""
+    if n_devices < 1:
+        raise ValueError("n_devices must be >= 1")
+    load = [0] * n_devices
+    out: List[List[int]] = [[] for _ in range(n_devices)]
+    for i in sorted(range(len(requests)), key=lambda k: (requests[k].arrival, k)):
+        d = min(range(n_devices), key=lambda k: (load[k], k))
+        out[d].append(i)
+        load[d] += requests[i].work
+    return out
 
 
 def device_work(requests: List[Request], device: int = 0, host_s_per_layer: float = 5e-4) -> List[float]:

@@ -115,6 +115,26 @@ def test_large_requests_are_the_same_alone_and_in_the_mix():
 
 
 @pytest.mark.gpu
+def test_one_server_over_a_device_list():
+    """The multi-device Server with one device: every request is admitted on
+    it and each result equals the single-device Server's."""
+    from mettleq_b200.serving import Server
+    a = _small_requests(8, seed=7)
+    b = _small_requests(8, seed=7)
+    s1 = Server(max_active=8, keep_states=True)
+    s2 = Server(max_active=8, keep_states=True, devices=[0])
+    try:
+        s1.serve(a, realtime=False)
+        s2.serve(b, realtime=False)
+        assert s2.served_on == {0: 8}
+        for x, y in zip(a, b):
+            assert np.array_equal(x.state, y.state) and np.array_equal(x.samples, y.samples)
+    finally:
+        s1.close()
+        s2.close()
+
+
+@pytest.mark.gpu
 def test_admission_stays_within_the_budget():
     from mettleq_b200.serving import Server
     reqs = _small_requests(20, seed=2)
