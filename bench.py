@@ -436,7 +436,8 @@ def run_batch(args, count=None, steps=None, device: int = 0, indices=None, plain
     t0 = time.perf_counter()
     tune = autotune([ns[i] for i in sub], [ds[i] for i in sub], packed_sub, device=device)
     tune_s = time.perf_counter() - t0
-    b = CircuitBatch(ns, ds, lanes=tune["lanes"], small_threads=tune["small_threads"], device=device)
+    b = CircuitBatch(ns, ds, lanes=tune["lanes"], small_threads=tune["small_threads"], device=device,
+                     tiles=tune.get("tiles"))
     packed = b.pack(mats)
     t0 = time.perf_counter()
     b.run(packed=packed)

@@ -203,6 +203,11 @@ int mq_batch_info(const mq_batch* b, uint64_t* mats_count, uint64_t* probs_count
  * circuit's full probability vector in order (first qubit = MSB); z0_dev
  * (device, float64): <Z_0> per circuit.  Asynchronous on the batch stream. */
 int mq_batch_run(mq_batch* b, const double* mats, float* probs_dev, double* z0_dev);
+/* The tile shape of the large circuits' sweeps (an autotuner's choice):
+ * largest tile in bits (0 = default, else 6..12), low passenger bits of a
+ * high sweep (-1 = default, else 0..5, fewer than tile_max), smallest tile
+ * (0 = default).  Only before the first mq_batch_run. */
+int mq_batch_set_tiles(mq_batch* b, int tile_max, int passengers, int tile_min);
 int mq_batch_sync(mq_batch* b);
 int mq_batch_destroy(mq_batch* b);
 

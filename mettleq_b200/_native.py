@@ -61,6 +61,7 @@ SIGNATURES = {
     "mq_batch_create": (_I, [_I, _P, _I, _P, _P, _P, _I, _I, C.POINTER(_P)]),
     "mq_batch_info": (_I, [_P, C.POINTER(_U64), C.POINTER(_U64), C.POINTER(_I), C.POINTER(_I)]),
     "mq_batch_run": (_I, [_P, _P, _P, _P]),
+    "mq_batch_set_tiles": (_I, [_P, _I, _I, _I]),
     "mq_batch_sync": (_I, [_P]),
     "mq_batch_destroy": (_I, [_P]),
     "mq_apply_pauli_sum": (_I, [_P, _P, _I, _P, _P, _P, _P]),

@@ -11,8 +11,9 @@ memory).  Outputs stay on the device: every circuit's probability vector
 (float32) and <Z_0> (float64).
 
 ``autotune`` picks the batch's launch shape (threads per block of the
-shared-memory kernel, number of parallel lanes) by timing the candidates on
-the batch itself.
+shared-memory kernel, number of parallel lanes) and then the tile shape of
+the large circuits' sweeps (largest tile, passenger bits, smallest tile) by
+timing the candidates on the batch itself.
 
 ``hea_batch`` generates the benchmark's batches: hardware-efficient ansatz
 circuits, RY and RZ angles U[-pi, pi] on every qubit per layer, then a CNOT
@@ -82,7 +83,8 @@ class CircuitBatch:
     launch (the first run also captures the graph)."""
 
     def __init__(self, n_qubits: Sequence[int], depths: Sequence[int], ladder=True, device: int = 0,
-                 lanes: int = 8, small_threads: int = 256, stream: Optional[int] = None):
+                 lanes: int = 8, small_threads: int = 256, stream: Optional[int] = None,
+                 tiles: Optional[Tuple[int, int, int]] = None):
         import torch  # device memory for the outputs (plumbing)
         self.n = [int(x) for x in n_qubits]
         self.depths = [int(x) for x in depths]
@@ -98,6 +100,9 @@ class CircuitBatch:
         N.check(self._lib.mq_batch_create(self.device, C.c_void_p(stream or 0), len(self.n), _ptr(ns), _ptr(ds),
                                           _ptr(lad), int(lanes), int(small_threads), C.byref(h)))
         self._h = h
+        self.tiles = tuple(int(x) for x in tiles) if tiles is not None else (0, -1, 0)
+        if tiles is not None:
+            N.check(self._lib.mq_batch_set_tiles(h, *self.tiles))
         mc, pc = C.c_uint64(), C.c_uint64()
         nsm, nlg = C.c_int(), C.c_int()
         N.check(self._lib.mq_batch_info(h, C.byref(mc), C.byref(pc), C.byref(nsm), C.byref(nlg)))
@@ -151,34 +156,58 @@ class CircuitBatch:
         return self.probs_dev[int(self.offsets[c]):int(self.offsets[c + 1])].cpu().numpy()
 
 
-def autotune(n_qubits: Sequence[int], depths: Sequence[int], packed: np.ndarray, device: int = 0,
-             lanes=(4, 8, 16), small_threads=(128, 256, 512), repeats: int = 2,
-             cache: Optional[Dict] = None) -> Dict[str, int]:
-    """Time every (lanes, small_threads) candidate on this batch (graph capture
-    excluded: each candidate runs once untimed) and return the fastest.
-    ``cache`` (a dict) memoises the choice per batch signature."""
+# Tile shapes (largest tile, low passenger bits, smallest tile) the autotuner
+# tries for the large circuits: the library default first, then smaller and
+# larger tiles and fewer / more passengers (shorter / longer contiguous runs).
+TILE_CANDIDATES = ((0, -1, 0), (11, 4, 0), (10, 4, 0), (12, 3, 0), (12, 5, 0), (12, 4, 12))
+
+
+def _time_batch(n_qubits, depths, packed, device, repeats, **kw) -> float:
     import torch
+    b = CircuitBatch(n_qubits, depths, device=device, **kw)
+    try:
+        b.run(packed=packed)  # captures the graph (untimed)
+        b.synchronize()
+        ts = []
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            b.run(packed=packed)
+            b.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return min(ts)
+    finally:
+        b.close()
+        torch.cuda.synchronize(device)
+
+
+def autotune(n_qubits: Sequence[int], depths: Sequence[int], packed: np.ndarray, device: int = 0,
+             lanes=(4, 8, 16), small_threads=(128, 256, 512), tiles=TILE_CANDIDATES, repeats: int = 2,
+             cache: Optional[Dict] = None) -> Dict:
+    """Choose the batch's launch shape and tile shape by timing them on this
+    batch (graph capture excluded: each candidate runs once untimed):
+    first every (lanes, small_threads) pair with the default tiles, then
+    every tile shape of ``tiles`` (largest tile, passengers, smallest tile)
+    for the large circuits' sweeps with the best pair.  Returns the choice
+    with the time of every tile candidate.  ``cache`` (a dict) memoises the
+    choice per batch signature."""
     key = (tuple(sorted(set(int(n) for n in n_qubits))), len(n_qubits), int(sum(depths)))
     if cache is not None and key in cache:
         return cache[key]
     best, best_t = None, float("inf")
     for nl, nt in itertools.product(lanes, small_threads):
-        b = CircuitBatch(n_qubits, depths, lanes=nl, small_threads=nt, device=device)
-        try:
-            b.run(packed=packed)
-            b.synchronize()
-            ts = []
-            for _ in range(repeats):
-                t0 = time.perf_counter()
-                b.run(packed=packed)
-                b.synchronize()
-                ts.append(time.perf_counter() - t0)
-            t = min(ts)
-        finally:
-            b.close()
-            torch.cuda.synchronize(device)
+        t = _time_batch(n_qubits, depths, packed, device, repeats, lanes=nl, small_threads=nt)
         if t < best_t:
             best, best_t = {"lanes": nl, "small_threads": nt}, t
+    tried = {}
+    best_tiles, best_tt = None, float("inf")
+    if any(int(n) > 13 for n in n_qubits):
+        for tl in tiles:
+            t = _time_batch(n_qubits, depths, packed, device, repeats, lanes=best["lanes"],
+                            small_threads=best["small_threads"], tiles=tl)
+            tried["%d/%d/%d" % tl] = t
+            if t < best_tt:
+                best_tiles, best_tt = tl, t
+    best = dict(best, tiles=best_tiles, tile_times_s=tried)
     if cache is not None:
         cache[key] = best
     return best

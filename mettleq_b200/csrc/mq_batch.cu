@@ -200,6 +200,8 @@ struct mq_batch {
   double* d_zpart = nullptr;
   uint32_t zblocks = 0;
   int num_sms = 148;
+  // sweep plan of the large circuits (mq_batch_set_tiles; 0 / -1 = defaults)
+  int tile_max = 0, tile_pas = -1, tile_min = 0;
   cudaGraphExec_t exec = nullptr;
   float* graph_probs = nullptr;
   double* graph_z0 = nullptr;
@@ -241,6 +243,9 @@ static int lane_state_for(mq_batch* b, int lane, int n, mq_state** out) {
   h->num_sms = b->num_sms;
   h->device_sms = b->num_sms;
   h->stream = b->lane_stream[lane];
+  h->tile_max = b->tile_max;
+  h->tile_pas = b->tile_pas;
+  h->tile_min = b->tile_min;
   h->state_bytes = (size_t(1) << n) * 8;
   cudaError_t e = cudaMalloc(&h->buf[0], h->state_bytes);
   if (e == cudaSuccess) e = cudaMalloc(&h->buf[1], h->state_bytes);
@@ -447,6 +452,19 @@ int mq_batch_info(const mq_batch* b, uint64_t* mats_count, uint64_t* probs_count
   if (probs_count) *probs_count = b->probs_total;
   if (n_small) *n_small = (int)b->small.size();
   if (n_large) *n_large = (int)b->large.size();
+  return MQ_OK;
+}
+
+int mq_batch_set_tiles(mq_batch* b, int tile_max, int passengers, int tile_min) {
+  if (!b) return fail(MQ_EINVAL, "null batch handle");
+  if (b->exec) return fail(MQ_EINVAL, "the tile plan is fixed once the batch has run (its graph is captured)");
+  if (tile_max != 0 && (tile_max < 6 || tile_max > 12)) return fail(MQ_EINVAL, "tile_max must be 0 or in [6, 12]");
+  if (passengers < -1 || passengers > 5) return fail(MQ_EINVAL, "passengers must be -1 or in [0, 5]");
+  if (tile_min < 0 || tile_min > 12) return fail(MQ_EINVAL, "tile_min must be 0 or in [1, 12]");
+  if (tile_max && passengers >= tile_max) return fail(MQ_EINVAL, "passengers must leave room for targets in a tile");
+  b->tile_max = tile_max;
+  b->tile_pas = passengers;
+  b->tile_min = tile_min;
   return MQ_OK;
 }
 

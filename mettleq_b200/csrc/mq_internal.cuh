@@ -195,6 +195,11 @@ struct mq_state {
   size_t scratch_bytes = 0;
   uint64_t launches = 0;
   uint64_t sweeps = 0;
+  // sweep plan of this handle (0 / -1: the process-wide defaults): largest
+  // tile (bits), low passenger bits of a high sweep, smallest tile
+  int tile_max = 0;
+  int tile_pas = -1;
+  int tile_min = 0;
 
   size_t amp_bytes() const { return dtype == MQ_C64 ? 8 : 16; }
   uint64_t dim() const { return uint64_t(1) << n; }

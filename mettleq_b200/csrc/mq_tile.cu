@@ -952,6 +952,14 @@ static bool euler_enabled(const mq_state* h) {
   return h->n >= env_int("MQ_EULER_MIN_QUBITS", 20, 1, 32);
 }
 static int min_tile() { return env_int("MQ_TILE_MIN", 10, 1, 12); }
+// The sweep plan of one handle: its own tile shape (mq_batch_set_tiles sets
+// one on a batch's states) or the process-wide defaults above.
+static int plan_tile_max(const mq_state* h) {
+  if (h->tile_max > 0) return std::min(h->tile_max, h->dtype == MQ_C64 ? 12 : 11);
+  return tile_max(h->dtype);
+}
+static int plan_passengers(const mq_state* h) { return h->tile_pas >= 0 ? h->tile_pas : passengers(); }
+static int plan_min_tile(const mq_state* h) { return h->tile_min > 0 ? h->tile_min : min_tile(); }
 // The Euler layer's sweeps fill their tiles to 12 bits with low passengers:
 // a 7-bit sweep then moves 256-byte runs (fused config layer at 30 qubits
 // 17.9 -> 16.3 ms); the complex sweeps measured slower that way.
@@ -962,9 +970,12 @@ static int euler_low_tile() { return env_int("MQ_EULER_LOW_TILE", 12, 1, 12); }
 // with one (three CTAs per SM).
 static int tile13_lt() { return env_int("MQ_TILE13_LT", 8, 8, 9); }
 // Euler layers: a high sweep of 8 target bits as a 13-bit tile with five
-// passengers (256-byte runs, one tile buffer) instead of a 12-bit one
-// (fused config layer at 27 qubits 1.94 -> 1.87 ms, at 30 qubits 15.6 -> 15.5 ms).
-static bool euler_hi13() { return env_int("MQ_EULER_HI13", 1, 0, 1) == 1; }
+// passengers (256-byte runs, one tile buffer) instead of a 12-bit one.  With
+// per-thread copies that paid (fused config layer at 30 qubits 15.6 -> 15.5
+// ms); with TMA tiles the 12-bit tile and its second buffer win (30 qubits
+// 14.07 -> 13.76 ms), so the default follows the tile movement.
+static bool tma_enabled();
+static bool euler_hi13() { return env_int("MQ_EULER_HI13", tma_enabled() ? 0 : 1, 0, 1) == 1; }
 // U(2) layers without diagonal terms through the Euler split as well.
 static bool euler_plain() { return env_int("MQ_EULER_PLAIN", 1, 0, 1) == 1; }
 // Euler layers: the high bit group (1 = the lowest) whose sweep carries the
@@ -1086,7 +1097,7 @@ static int launch_tile_t(mq_state* h, PT& P, size_t smem, bool out_of_place) {
 // per-thread asynchronous copies.
 template <typename R, int M, int LR, int LT, int MODE, typename PT>
 static int launch_tile_sel(mq_state* h, PT& P, size_t smem, bool oop) {
-  if constexpr (M >= 10 && LR == 4 && LT <= 8) {
+  if constexpr (M >= 10 && LR == 4) {
     if (P.tma.ndim) return launch_tile_t<R, M, LR, LT, MODE, PT, true>(h, P, smem, oop);
   }
   return launch_tile_t<R, M, LR, LT, MODE, PT, false>(h, P, smem, oop);
@@ -1321,7 +1332,7 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
                      const EpiPlan* epi = nullptr) {
   const int m = (int)sw.tile_bits.size();
   const int lr = epi ? std::min(m, 4) : reg_bits(h->dtype, m);
-  if (m < 1 || m > std::max(tile_max(h->dtype), h->dtype == MQ_C64 && lr == 4 ? kTileMaxC64 : 0) || m > h->n)
+  if (m < 1 || m > std::max(plan_tile_max(h), h->dtype == MQ_C64 && lr == 4 ? kTileMaxC64 : 0) || m > h->n)
     return fail(MQ_EINVAL, "bad tile size");
   if (sw.tile_bits[0] != 0) return fail(MQ_EINVAL, "tile must contain index bit 0");
   if ((int)sw.ops.size() > kMaxOps || (int)sw.phases.size() > kMaxPhases) return fail(MQ_EINVAL, "tile plan too large");
@@ -1550,8 +1561,8 @@ static bool build_u2_sweep(mq_state* h, const double* mats, const uint8_t* activ
   if (gbits.empty()) return false;
   // a caller's minimum above the planner's maximum (13-bit complex64 tiles)
   // raises the maximum with it
-  const int tmax = (h->dtype == MQ_C64 && tmin > tile_max(h->dtype)) ? std::min(tmin, kTileMaxC64) : tile_max(h->dtype);
-  sw.tile_bits = tile_for(n, gbits, passengers(), tmax, tmin > 0 ? tmin : min_tile());
+  const int tmax = (h->dtype == MQ_C64 && tmin > plan_tile_max(h)) ? std::min(tmin, kTileMaxC64) : plan_tile_max(h);
+  sw.tile_bits = tile_for(n, gbits, plan_passengers(h), tmax, tmin > 0 ? tmin : plan_min_tile(h));
   const int m = (int)sw.tile_bits.size();
   const int lr = reg_bits(h->dtype, m);
   std::vector<int> order;
@@ -1579,7 +1590,7 @@ int launch_u2_layer(mq_state* h, const double* mats, const uint8_t* active) {
       for (int q = 0; q < h->n; ++q) all = all && active[q];
     if (all) return launch_layer(h, mats, nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0);
   }
-  for (auto [start, cnt] : split_bits(h->n, tile_max(h->dtype), passengers())) {
+  for (auto [start, cnt] : split_bits(h->n, plan_tile_max(h), plan_passengers(h))) {
     Sweep sw;
     std::vector<int> op_phase, op_rk;
     if (!build_u2_sweep(h, mats, active, start, cnt, sw, op_phase, op_rk)) continue;
@@ -1645,7 +1656,7 @@ static int launch_layer_euler(mq_state* h, const double* mats, int n_terms, cons
   }
   post_k.push_back(MQ_DIAG_GLOBAL); post_w.push_back(0); post_w.push_back(-1);
   post_p.push_back(alpha_sum); post_p.insert(post_p.end(), 7, 0.0);
-  const auto groups = split_bits(n, tile_max(h->dtype), passengers());
+  const auto groups = split_bits(n, plan_tile_max(h), plan_passengers(h));
   const int max_entries = kEpiLutBytes / (int)h->amp_bytes();
   // RY sweeps in tangent form: the product of the factors they leave out
   // rides on the low sweep's register diagonal
@@ -1769,13 +1780,13 @@ int launch_layer(mq_state* h, const double* mats, const uint8_t* active, int n_t
     int rc = launch_layer_euler(h, mats, n_terms, kinds, wires, params, cols, c, &done);
     if (rc || done) return rc;
   }
-  const auto groups = split_bits(n, tile_max(h->dtype), passengers());
+  const auto groups = split_bits(n, plan_tile_max(h), plan_passengers(h));
   // low sweep plan first, so that argument errors surface before any launch
   Sweep low;
   std::vector<int> low_phase, low_rk;
   const bool low_u2 = u2 && build_u2_sweep(h, mats, active, groups[0].first, groups[0].second, low, low_phase, low_rk,
                                            mats_dev);
-  if (!low_u2) low.tile_bits = tile_for(n, {0}, passengers(), tile_max(h->dtype), min_tile());
+  if (!low_u2) low.tile_bits = tile_for(n, {0}, plan_passengers(h), plan_tile_max(h), plan_min_tile(h));
   const int m = (int)low.tile_bits.size();
   EpiPlan e;
   if (n_terms > 0) {
@@ -1838,8 +1849,8 @@ int launch_qft_stages(mq_state* h, int q0, int k, int j_begin, int j_end, int in
   const int n = h->n;
   if (k <= 0 || j_begin >= j_end) return MQ_OK;
   if (q0 < 0 || q0 + k > n || j_begin < 0 || j_end > k) return fail(MQ_EINVAL, "invalid QFT stage range");
-  const int tmax = tile_max(h->dtype);
-  const int pas = passengers();
+  const int tmax = plan_tile_max(h);
+  const int pas = plan_passengers(h);
   const int lad_shift = n - q0 - k;  // index bit of the last wire
   // stage j acts on bit b_j = n-1-q0-j.  Groups of consecutive stages: the
   // lowest group may reach bit 0 (tmax bits), the others hold tmax - pas.
@@ -1874,7 +1885,7 @@ int launch_qft_stages(mq_state* h, int q0, int k, int j_begin, int j_end, int in
     std::vector<int> gbits;
     for (int j : stages) gbits.push_back(n - 1 - q0 - j);
     Sweep sw;
-    sw.tile_bits = tile_for(n, gbits, pas, tmax, min_tile());
+    sw.tile_bits = tile_for(n, gbits, pas, tmax, plan_min_tile(h));
     const int m = (int)sw.tile_bits.size();
     if (m > tmax) return fail(MQ_EINVAL, "qft tile too large");
     const int lr = reg_bits(h->dtype, m);
@@ -1910,8 +1921,8 @@ int launch_qft_contiguous(mq_state* h, int q0, int k, int inverse) {
 // starts a new sweep, so the list order is respected.
 int launch_cu2_list(mq_state* h, int n_gates, const int32_t* targets, const uint32_t* cmasks, const double* mats) {
   const int n = h->n;
-  const int tmax = tile_max(h->dtype);
-  const int pas = passengers();
+  const int tmax = plan_tile_max(h);
+  const int pas = plan_passengers(h);
   int g = 0;
   while (g < n_gates) {
     std::vector<int> members;
@@ -1927,7 +1938,7 @@ int launch_cu2_list(mq_state* h, int n_gates, const int32_t* targets, const uint
     std::vector<int> gbits;
     for (int i : members) gbits.push_back(n - 1 - targets[i]);
     Sweep sw;
-    sw.tile_bits = tile_for(n, gbits, pas, tmax, min_tile());
+    sw.tile_bits = tile_for(n, gbits, pas, tmax, plan_min_tile(h));
     const int m = (int)sw.tile_bits.size();
     if (m > tmax) return fail(MQ_EINVAL, "controlled-gate tile too large");
     const int lr = reg_bits(h->dtype, m);

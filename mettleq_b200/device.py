@@ -106,6 +106,8 @@ class Device:
             sim.apply_qft(layer["wires"], inverse=layer.get("inverse", False))
         elif name == "_CULIST":
             sim.apply_controlled(layer["gates"])
+        elif name == "_PAIRLAYER":
+            sim.apply_pauli_pair_layer(layer["kind"], layer["bonds"], layer["thetas"])
         else:
             raise ValueError(f"Unknown fused layer: {name}")
 

@@ -314,6 +314,38 @@ class StateVector:
         """CPHASE(theta_b) per bond, CZ = pi (diag_weighted_layer, diag.py:123-167)."""
         self._diag_layer(N.MQ_DIAG_CPHASE, bonds, thetas)
 
+    def apply_pauli_pair_layer(self, kind: str, bonds: Sequence[Tuple[int, int]], thetas: Sequence[float]) -> None:
+        """exp(-i sum_b theta_b P_a P_b) for P = X (kind "XX") or Y ("YY"),
+        the native XXPHASE / YYPHASE without the 1/2 (xx_layer / yy_layer,
+        shaders/pauli_pair.py:32-64).  The terms of one family commute, so
+        with U = H (X = H Z H) or U = S H (Y = U Z U^+) the layer is U on the
+        bonds' wires after the ZZ layer after U^+: one fused layer (the U^+
+        sweeps carry the ZZ terms in their last register phase) and one U(2)
+        layer."""
+        bonds = [(int(a), int(b)) for a, b in bonds]
+        thetas = [float(t) for t in thetas]
+        if len(bonds) != len(thetas):
+            raise ValueError("bonds/thetas length mismatch")
+        if not bonds:
+            return
+        h = np.array([[1, 1], [1, -1]], dtype=np.complex128) / math.sqrt(2.0)
+        if kind == "XX":
+            u = h
+        elif kind == "YY":
+            u = np.array([[1, 0], [0, 1j]], dtype=np.complex128) @ h
+        else:
+            raise ValueError("kind must be 'XX' or 'YY'")
+        wires = sorted({w for b in bonds for w in b})
+        pre = np.tile(np.eye(2, dtype=np.complex128).reshape(1, 4), (self.n, 1))
+        post = pre.copy()
+        for w in wires:
+            if not (0 <= w < self.n):
+                raise ValueError("Qubit index out of range")
+            pre[w] = u.conj().T.reshape(4)
+            post[w] = u.reshape(4)
+        self.apply_layer(pre, wires, [(N.MQ_DIAG_ZZ, a, b, [t]) for (a, b), t in zip(bonds, thetas)])
+        self.apply_u2_layer(post, wires)
+
     def _diag_layer(self, kind: int, bonds, thetas) -> None:
         bonds = list(bonds)
         thetas = list(thetas)

@@ -20,9 +20,11 @@ execute, with the detection semantics of the reference's
 * CH/CRX/CRY/Toffoli runs become controlled-U(2) lists (device.py:756-806).
 
 Composite gates are rewritten first: ISWAP = diag(1,i,i,1) then SWAP
-(device.py:1233-1236); XXPHASE/YYPHASE = basis change around ZZPHASE (the
-H/S conjugation of shaders/pauli_pair.py:32-64); FREDKIN = CNOT(b,a)
-TOFFOLI(c,a,b) CNOT(b,a).
+(device.py:1233-1236); FREDKIN = CNOT(b,a) TOFFOLI(c,a,b) CNOT(b,a).  Runs
+of XXPHASE (or of YYPHASE) terms become one ``_PAIRLAYER``: the basis change
+H (or V = S H) on their wires around one ZZ layer (the conjugation of
+shaders/pauli_pair.py:32-64), which the engine runs as one fused layer (the
+basis change's sweeps carrying the ZZ terms) and one U(2) layer.
 """
 from __future__ import annotations
 
@@ -93,12 +95,9 @@ def decompose(ops: Sequence[dict]) -> List[dict]:
             out.append({"name": "_D2", "wires": list(w), "diag": [1, 1j, 1j, 1]})
             out.append({"name": "SWAP", "wires": list(w), "parameters": []})
         elif name in ("XXPHASE", "YYPHASE"):
-            u = G.single_qubit_matrix("H") if name == "XXPHASE" else _V
-            for q in w:
-                out.append({"name": "_M1", "wires": [q], "matrix": u.conj().T})
-            out.append({"name": "ZZPHASE", "wires": list(w), "parameters": [p[0]]})
-            for q in w:
-                out.append({"name": "_M1", "wires": [q], "matrix": u})
+            # a pair term; runs of one family become one _PAIRLAYER
+            out.append({"name": "_XXPAIR" if name == "XXPHASE" else "_YYPAIR", "wires": list(w),
+                        "parameters": [p[0]]})
         elif name == "FREDKIN":
             c, a, b = w
             out.append({"name": "CNOT", "wires": [b, a], "parameters": []})
@@ -372,6 +371,20 @@ def fuse(operations: Sequence[dict], n: int, *, schedule: bool = True) -> List[D
             fused.append({"name": "_XORLAYER", "rows": rows, "c": c})
             i = j
             continue
+        if name in ("_XXPAIR", "_YYPAIR"):
+            # exp(-i sum_b t_b P_a P_b), P = X or Y: the terms of one family
+            # commute, so the run is one basis change around one ZZ layer
+            # (shaders/pauli_pair.py:32-64)
+            bonds, thetas = [], []
+            j = i
+            while j < N and ops[j]["name"] == name:
+                bonds.append(tuple(ops[j]["wires"]))
+                thetas.append(float(ops[j]["parameters"][0]))
+                j += 1
+            fused.append({"name": "_PAIRLAYER", "kind": "XX" if name == "_XXPAIR" else "YY",
+                          "bonds": bonds, "thetas": thetas})
+            i = j
+            continue
         if name in CONTROLLED:
             gates = []
             j = i
@@ -546,6 +559,9 @@ def expected_sweeps(layer: dict, n: int, dtype: str = "complex64") -> int:
         return hi + 1 + extra
     if name in ("_DIAG", "_XORLAYER"):
         return 1
+    if name == "_PAIRLAYER":
+        wires = sorted({w for b in layer["bonds"] for w in b})
+        return 2 * u2_sweeps(wires)
     if name == "_QFTSTAGES":
         cnt = layer["j_end"] - layer["j_begin"]
         return 1 if cnt + pas <= tmax else -(-cnt // (tmax - pas))

@@ -336,6 +336,11 @@ class ShardedState:
                 pending.append(("CNOT", self.pos[cq], self.pos[tq]))
         self._flush_affine(pending)
 
+    def apply_qft(self, wires=None, inverse: bool = False) -> None:
+        raise NotImplementedError(
+            "QFT layers on a sharded state are not supported: their stages on global qubits need a global/local "
+            "swap before the stage sweeps, which is not built")
+
     def apply_layer(self, mats=None, active=None, terms=(), rows=None, c: int = 0) -> None:
         """U(2) layer, then diagonal terms, then permutation (the order of
         ``StateVector.apply_layer``)."""

@@ -91,3 +91,46 @@ def test_batch_without_ladder_and_plain_path_agree():
             assert np.max(np.abs(b.probabilities(c) - plain)) < 2e-6
     finally:
         b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tiles", [(11, 4, 0), (10, 4, 0), (12, 3, 0), (12, 5, 0), (12, 4, 12), (8, 2, 6)])
+def test_batch_tile_shapes_match_oracle(tiles):
+    """Every tile shape the autotuner may choose gives the oracle's results
+    (the large circuits' sweeps re-planned with that shape)."""
+    from mettleq_b200.batch import CircuitBatch
+    rng = np.random.default_rng(sum(tiles))
+    ns = [14, 15, 17, 19, 20, 9]
+    ds = [3, 2, 2, 3, 2, 2]
+    params = [rng.uniform(-math.pi, math.pi, size=(d, n, 2)) for n, d in zip(ns, ds)]
+    b = CircuitBatch(ns, ds, lanes=2, tiles=tiles)
+    try:
+        b.run([hea_mats(p) for p in params])
+        z0 = b.z0()
+        for c, p in enumerate(params):
+            ref_p, ref_z = oracle_run(p)
+            assert np.max(np.abs(b.probabilities(c) - ref_p)) < 2e-6, (tiles, ns[c])
+            assert abs(z0[c] - ref_z) < 1e-5
+    finally:
+        b.close()
+
+
+@pytest.mark.gpu
+def test_autotune_chooses_a_launch_and_tile_shape():
+    from mettleq_b200.batch import TILE_CANDIDATES, CircuitBatch, autotune
+    ns, ds, ps = hea_batch(24, seed=4)
+    b = CircuitBatch(ns, ds)
+    packed = b.pack([hea_mats(p) for p in ps])
+    b.close()
+    choice = autotune(ns, ds, packed, lanes=(2, 4), small_threads=(256,), repeats=1)
+    assert choice["lanes"] in (2, 4) and choice["small_threads"] == 256
+    assert tuple(choice["tiles"]) in TILE_CANDIDATES
+    assert len(choice["tile_times_s"]) == len(TILE_CANDIDATES)
+    b2 = CircuitBatch(ns, ds, lanes=choice["lanes"], tiles=choice["tiles"])
+    try:
+        b2.run(packed=packed)
+        z0 = b2.z0()
+        for c in (0, len(ns) - 1):
+            assert abs(z0[c] - oracle_run(ps[c])[1]) < 1e-5
+    finally:
+        b2.close()

@@ -50,9 +50,36 @@ def interpret(layers, n, vec):
         elif name == "_CULIST":
             for cs, t, u in L["gates"]:
                 o.apply_multi_controlled_single(u, cs, t)
+        elif name == "_PAIRLAYER":
+            for (a, b), t in zip(L["bonds"], L["thetas"]):
+                (o.apply_xx_phase if L["kind"] == "XX" else o.apply_yy_phase)(t, a, b)
         else:
             raise AssertionError(name)
     return o.state
+
+
+def test_pair_terms_fuse_into_one_layer_per_family_run():
+    """Runs of XXPHASE (YYPHASE) terms, even on overlapping bonds, become one
+    _PAIRLAYER; the two families are not merged (X and Y on one qubit do not
+    commute), and the result equals the gate stream's."""
+    n = 7
+    rng = np.random.default_rng(3)
+    ops = [{"name": "XXPHASE", "wires": [i, i + 1], "parameters": [float(rng.uniform(-1, 1))]} for i in range(n - 1)]
+    ops += [{"name": "XXPHASE", "wires": [0, 5], "parameters": [0.3]}]
+    ops += [{"name": "YYPHASE", "wires": [i, (i + 2) % n], "parameters": [float(rng.uniform(-1, 1))]}
+            for i in range(n)]
+    ops += [{"name": "RX", "wires": [2], "parameters": [0.4]}]
+    ops += [{"name": "XXPHASE", "wires": [1, 3], "parameters": [0.2]}]
+    layers = F.fuse(ops, n)
+    pairs = [L for L in layers if L["name"] == "_PAIRLAYER"]
+    assert [p["kind"] for p in pairs] == ["XX", "YY", "XX"]
+    assert len(pairs[0]["bonds"]) == n and len(pairs[1]["bonds"]) == n
+    vec = rand_state(n, 4, np.complex128)
+    assert np.max(np.abs(interpret(layers, n, vec) - reference(ops, n, vec))) < 1e-12
+    # at 30 qubits a chain over every qubit is two U(2) layers: 2 x 4 sweeps
+    chain = {"name": "_PAIRLAYER", "kind": "XX", "bonds": [(i, i + 1) for i in range(29)], "thetas": [0.1] * 29}
+    assert F.expected_sweeps(chain, 30) == 8
+    assert F.expected_sweeps(pairs[0], 30) == 2  # wires 0..6: the top bit group only
 
 
 def reference(ops, n, vec):

@@ -457,3 +457,33 @@ def test_device_shots_agree_with_reference_probabilities():
         exp = np.append(probs[keep] * 1000, probs[~keep].sum() * 1000)
         stat = float(np.sum((obs - exp) ** 2 / exp))
         assert chi2.sf(stat, obs.size - 1) > 1e-3, seed
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [np.complex64, np.complex128])
+@pytest.mark.parametrize("kind", ["XX", "YY"])
+@pytest.mark.parametrize("n", [6, 16, 22])
+def test_pauli_pair_layer(n, kind, dtype):
+    """exp(-i sum_b t_b P_a P_b) (xx_layer / yy_layer, shaders/pauli_pair.py
+    :32-64) over a chain and long-range bonds, against the oracle's per-bond
+    anti-diagonal passes (sim.py:226-258); also through Device.execute."""
+    from mettleq_b200.device import Device
+    rng = np.random.default_rng(300 + n)
+    bonds = [(i, i + 1) for i in range(n - 1)] + [(0, n - 1), (1, n // 2)]
+    thetas = rng.uniform(-math.pi, math.pi, len(bonds))
+    vec = rand_state(n, 9, dtype)
+    sv = _sv(n, dtype, vec)
+    sv.apply_pauli_pair_layer(kind, bonds, thetas)
+    o = _oracle(n, np.complex128, vec)
+    for (a, b), t in zip(bonds, thetas):
+        (o.apply_xx_phase if kind == "XX" else o.apply_yy_phase)(float(t), a, b)
+    assert _err(sv.get(), o.state) <= TOL[dtype]
+    sv.close()
+    ops = [{"name": kind + "PHASE", "wires": [a, b], "parameters": [float(t)]} for (a, b), t in zip(bonds, thetas)]
+    dev = Device(n, dtype=np.dtype(dtype).name)
+    try:
+        dev.sim.set(vec)
+        dev.execute(ops)
+        assert _err(dev.statevector(), o.state) <= TOL[dtype]
+    finally:
+        dev.close()
