@@ -61,6 +61,7 @@ struct AdjPhase {
 };
 
 struct AdjParams {
+  TmaDesc tma;  // TMA form: src = psi, dst = lam (both swept in place)
   uint32_t n_tiles;
   uint8_t n, m, n_phases, store_psi;
   uint8_t tile_bit[16];
@@ -138,10 +139,17 @@ __device__ __forceinline__ uint32_t xsel(int r, const uint32_t* g) {
   return o;
 }
 
+// set when an adjoint sweep was abandoned (read and cleared by mq_sync)
+__device__ unsigned int g_adj_fault;
+
 // Tiles of 2^M amplitudes of psi and lam, 2^LT threads, shared-memory layout
 // as k_tile (chunk c at slot c ^ ((c >> 3) & 7)); per-block gradient partials
-// (one double per phase slot and step) go to `partials`.
-template <typename R, int M, int LR, int LT>
+// (one double per phase slot and step) go to `partials`.  TMA: thread 0 loads
+// a tile of both states as two boxes completing on one mbarrier per buffer
+// pair, and writes them back as two TMA stores; every wait is bounded
+// (kTmaWaitNs), and a CTA whose tile does not arrive sets g_adj_fault and
+// returns as a whole.
+template <typename R, int M, int LR, int LT, bool TMA>
 __global__ void __launch_bounds__(1 << LT)
 k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __restrict__ partials) {
   using T = V2<R>;
@@ -155,11 +163,24 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
   constexpr int LCH = (M - CB) - LT;
   static_assert(GPT >= 1 && CPT >= 1, "bad tile configuration");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* bufs = reinterpret_cast<T*>(smem_raw);  // [psi0, psi1, lam0, lam1]
+  // TMA: buffers on a 1024-byte boundary (the 128-byte swizzle), then the two
+  // mbarriers (the host adds the slack)
+  unsigned char* smem = smem_raw;
+  if constexpr (TMA) smem += (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
+  T* bufs = reinterpret_cast<T*>(smem);  // [psi0, psi1, lam0, lam1]
+  const uint32_t bar0 = smem_u32(smem + 4 * sizeof(T) * E);
   constexpr int WS = NT < 32 ? NT : 32;  // lanes per warp in use
   constexpr unsigned WMASK = WS == 32 ? 0xffffffffu : ((1u << WS) - 1u);
   __shared__ double red[(NT + 31) / 32][kAdjPartials];
   const int tid = threadIdx.x;
+  if constexpr (TMA) {
+    if (tid == 0) {
+      mbar_init(bar0, 1);
+      mbar_init(bar0 + 8u, 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+  }
   uint32_t g_t = 0;
 #pragma unroll
   for (int b = 0; b < LT; ++b)
@@ -197,19 +218,51 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
 #pragma unroll
     for (int k = 0; k < LR; ++k) acc[p][k][0] = acc[p][k][1] = acc[p][k][2] = 0;
 
+  // TMA (thread 0): the tile's psi and lam boxes into buffer pair `which`
+  auto tma_coords = [&](uint32_t base, int32_t (&c)[5]) {
+#pragma unroll
+    for (int d = 0; d < 5; ++d) c[d] = (int32_t)((base >> P.tma.start[d]) & P.tma.mask[d]);
+  };
+  auto tma_issue = [&](uint32_t tile, int which) {
+    int32_t c[5];
+    tma_coords(base_of(tile), c);
+    const uint32_t bar = bar0 + 8u * (uint32_t)which;
+    mbar_expect_tx(bar, 2u * P.tma.bytes);
+    tma_load_5d(smem_u32(bufs + which * E), &P.tma.src, c, bar);
+    tma_load_5d(smem_u32(bufs + (2 + which) * E), &P.tma.dst, c, bar);
+  };
+
   uint32_t tile = blockIdx.x;
-  if (tile < P.n_tiles) issue(tile, 0);
-  cp_async_commit();
+  if constexpr (TMA) {
+    if (tid == 0 && tile < P.n_tiles) tma_issue(tile, 0);
+  } else {
+    if (tile < P.n_tiles) issue(tile, 0);
+    cp_async_commit();
+  }
   T a[NR], b[NR];
   for (int it = 0; tile < P.n_tiles; tile += gridDim.x, ++it) {
     const int cb = it & 1;
     T* cp = bufs + cb * E;
     T* cl = bufs + (2 + cb) * E;
     const uint32_t next = tile + gridDim.x;
-    if (next < P.n_tiles) issue(next, cb ^ 1);
-    cp_async_commit();
-    cp_async_wait<1>();
-    __syncthreads();
+    if constexpr (TMA) {
+      const uint32_t bar = bar0 + 8u * (uint32_t)cb;
+      const uint32_t parity = (uint32_t)((it >> 1) & 1);
+      const bool ok = mbar_wait_bounded(bar, parity, kTmaWaitNs);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          atomicOr(&g_adj_fault, 1u);
+          mbar_wait_bounded(bar, parity, kTmaWaitNs);  // the load in flight, once more
+          bulk_wait_all();
+        }
+        return;
+      }
+    } else {
+      if (next < P.n_tiles) issue(next, cb ^ 1);
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncthreads();
+    }
 #pragma unroll
     for (int ph = 0; ph < MAXPH; ++ph) {
       if (ph >= P.n_phases) break;
@@ -239,7 +292,29 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
           cl[sq ^ xsel<LR>(r, sreg)] = b[r];
         }
       }
+      // TMA: the tile's last shared-memory writes become visible to the
+      // async proxy (the stores that read them, the load that overwrites)
+      if constexpr (TMA)
+        if (ph == P.n_phases - 1) fence_proxy_async_smem();
       __syncthreads();
+      if constexpr (TMA) {
+        // every thread has finished the previous tile: its buffer pair takes
+        // this CTA's next tile once the stores from it have read it out
+        if (ph == 0 && tid == 0 && next < P.n_tiles) {
+          bulk_wait_read();
+          tma_issue(next, cb ^ 1);
+        }
+      }
+    }
+    if constexpr (TMA) {
+      if (tid == 0) {
+        int32_t c[5];
+        tma_coords(base_of(tile), c);
+        if (P.store_psi) tma_store_5d(&P.tma.src, c, smem_u32(cp));
+        tma_store_5d(&P.tma.dst, c, smem_u32(cl));
+        bulk_commit();
+      }
+      continue;
     }
     const uint32_t gb = base_of(tile) | g_t;
     const float4* p4 = reinterpret_cast<const float4*>(cp);
@@ -251,7 +326,11 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
     }
     __syncthreads();
   }
-  cp_async_wait<0>();
+  if constexpr (TMA) {
+    if (tid == 0) bulk_wait_all();  // the last stores have written global memory
+  } else {
+    cp_async_wait<0>();
+  }
   // deterministic block reduction: lanes (xor tree), then warps in order
   const int lane = tid & 31, warp = tid >> 5;
   for (int j = tid; j < (NT + 31) / 32 * kAdjPartials; j += NT) (&red[0][0])[j] = 0.0;
@@ -271,7 +350,7 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
   for (int j = tid; j < kAdjPartials; j += NT) {
     double v = 0.0;
     for (int w = 0; w < (NT + 31) / 32; ++w) v = __dadd_rn(v, red[w][j]);
-    partials[(size_t)blockIdx.x * kAdjPartials + j] = v;
+    partials[(size_t)j * gridDim.x + blockIdx.x] = v;  // value-major: the collect reads runs
   }
 }
 
@@ -318,20 +397,33 @@ __global__ void __launch_bounds__(256) k_dot(const V2<R>* __restrict__ psi, cons
   }
 }
 
-// out[index[j/3]*3 + j%3] = sum over blocks b (in order) of partials[b][j]
-// for every (slot, Pauli) j whose slot carries a target.
+// out[index[j/3]*3 + j%3] = sum over blocks b of partials[j][b] (a fixed
+// order) for every (slot, Pauli) j whose slot carries a target.
 struct AdjCollect {
   int32_t index[kAdjSlots];
 };
-__global__ void k_adj_collect(const double* __restrict__ partials, uint32_t nblocks, const __grid_constant__ AdjCollect C,
-                              double* __restrict__ out) {
-  const int j = threadIdx.x;
-  if (j >= kAdjPartials) return;
+// One block per value j (partials[j * nblocks + b]): each thread sums a
+// strided set of blocks in increasing b, then a fixed halving tree; the
+// order depends only on nblocks, so results are reproducible.
+constexpr int kCollectThreads = 128;
+__global__ void __launch_bounds__(kCollectThreads)
+k_adj_collect(const double* __restrict__ partials, uint32_t nblocks, const __grid_constant__ AdjCollect C,
+              double* __restrict__ out) {
+  const int j = blockIdx.x;
   const int t = C.index[j / 3];
-  if (t < 0) return;
+  if (t < 0) return;  // the whole block: j is uniform
+  __shared__ double red[kCollectThreads];
   double v = 0.0;
-  for (uint32_t b = 0; b < nblocks; ++b) v = __dadd_rn(v, partials[(size_t)b * kAdjPartials + j]);
-  out[t * 3 + j % 3] = v;
+  const double* p = partials + (size_t)j * nblocks;
+  for (uint32_t b = threadIdx.x; b < nblocks; b += kCollectThreads) v = __dadd_rn(v, p[b]);
+  red[threadIdx.x] = v;
+  __syncthreads();
+#pragma unroll
+  for (int s = kCollectThreads / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] = __dadd_rn(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[t * 3 + j % 3] = red[0];
 }
 
 // ================================================================ host side
@@ -344,10 +436,29 @@ struct AdjTarget {
   double u[8];
 };
 
-template <typename R, int M, int LR, int LT>
-static int launch_adj_t(mq_state* psi, mq_state* lam, const AdjParams& P, double* partials, uint32_t* grid_out) {
-  auto kern = k_adj<R, M, LR, LT>;
-  const size_t smem = 4 * sizeof(V2<R>) * (size_t(1) << M);
+int take_adj_fault(mq_state* h, bool* fault) {
+  unsigned int v = 0;
+  MQ_CUDA(cudaMemcpyFromSymbolAsync(&v, g_adj_fault, sizeof(v), 0, cudaMemcpyDeviceToHost, h->stream));
+  MQ_CUDA(cudaStreamSynchronize(h->stream));
+  *fault = v != 0;
+  if (v) {
+    const unsigned int zero = 0;
+    MQ_CUDA(cudaMemcpyToSymbolAsync(g_adj_fault, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, h->stream));
+    MQ_CUDA(cudaStreamSynchronize(h->stream));
+  }
+  return MQ_OK;
+}
+
+template <typename R, int M, int LR, int LT, bool TMA>
+static int launch_adj_t(mq_state* psi, mq_state* lam, const AdjParams& P0, double* partials, uint32_t* grid_out) {
+  auto kern = k_adj<R, M, LR, LT, TMA>;
+  size_t smem = 4 * sizeof(V2<R>) * (size_t(1) << M);
+  AdjParams P = P0;
+  if constexpr (TMA) {
+    smem += 1024 + 64;  // 1024-byte alignment of the buffers, the mbarriers
+    int rc = encode_tile_maps(P.tma, psi->cur_buf(), lam->cur_buf());
+    if (rc) return rc;
+  }
   // one shared-memory size per instance: configure it once
   static std::mutex mu;
   static int configured = -1, bps_cached = 0;
@@ -387,7 +498,10 @@ static int dispatch_adj_lr(mq_state* psi, mq_state* lam, const AdjParams& P, dou
       constexpr int L = (MM) < LRT ? (MM) : LRT;                                     \
       constexpr int LTMAX = LRT == 3 ? 8 : 7;                                        \
       constexpr int LT = ((MM) - L) < LTMAX ? ((MM) - L) : LTMAX;                    \
-      return launch_adj_t<R, MM, L, LT>(psi, lam, P, partials, grid);                \
+      if constexpr ((MM) >= 10) {                                                    \
+        if (P.tma.ndim) return launch_adj_t<R, MM, L, LT, true>(psi, lam, P, partials, grid); \
+      }                                                                              \
+      return launch_adj_t<R, MM, L, LT, false>(psi, lam, P, partials, grid);         \
     }
     MQ_ADJ_CASE(1) MQ_ADJ_CASE(2) MQ_ADJ_CASE(3) MQ_ADJ_CASE(4) MQ_ADJ_CASE(5) MQ_ADJ_CASE(6)
     MQ_ADJ_CASE(7) MQ_ADJ_CASE(8) MQ_ADJ_CASE(9) MQ_ADJ_CASE(10) MQ_ADJ_CASE(11)
@@ -427,6 +541,10 @@ static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
   P.store_psi = store_psi ? 1 : 0;
   for (int k = 0; k < m; ++k) P.tile_bit[k] = (uint8_t)tile_bits[k];
   make_base_runs(P.runs, n, P.tile_bit, m);
+  // TMA form for tiles of 10 bits and more (both states move by TMA boxes)
+  if (tma_enabled() && m >= 10) {
+    if (plan_tma(n, psi->amp_bytes(), tile_bits, P.tma)) P.tma.store = 1;
+  }
   {
     const int cb = c64 ? 1 : 0;
     const int lt = std::min(lrt == 3 ? 8 : 7, m - lr);
@@ -478,7 +596,7 @@ static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
   if (!grads_dev) return MQ_OK;
   AdjCollect C;
   for (int sl = 0; sl < kAdjSlots; ++sl) C.index[sl] = slot_target[sl] < 0 ? -1 : index[slot_target[sl]];
-  k_adj_collect<<<1, kAdjPartials, 0, psi->stream>>>(partials, grid, C, grads_dev);
+  k_adj_collect<<<kAdjPartials, kCollectThreads, 0, psi->stream>>>(partials, grid, C, grads_dev);
   MQ_LAUNCHED("k_adj_collect");
   psi->launches += 1;
   return MQ_OK;

@@ -1,6 +1,7 @@
 // Internal definitions shared by the libmq CUDA sources (not part of the ABI).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
@@ -109,6 +110,32 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
+
+// ---------------------------------------------------------------- TMA tiles
+// TMA form of a sweep's tile movement (k_tile, k_adj).  The state is viewed
+// as a tensor of 8-byte words (complex64: one amplitude; complex128: its real
+// or imaginary part, word bit 0) whose dimensions are runs of index bits in
+// ascending order: dimension 0 is word bits [0, 4) (128 bytes), then
+// alternately runs of tile bits (box = the whole run, split at 8 bits) and
+// runs of free bits (box 1; coordinate = the tile base's bits there).  A tile
+// is then one box, and the tensor map's 128-byte swizzle puts 16-byte chunk j
+// of 128-byte row r at chunk j ^ (r & 7): the chunk layout the register
+// phases use, so they read TMA-loaded tiles unchanged.
+struct alignas(64) TmaDesc {
+  CUtensorMap src;     // over the buffer the sweep reads (k_adj: psi)
+  CUtensorMap dst;     // over the buffer it writes, the same one in place (k_adj: lam)
+  uint32_t bytes;      // one tile: the transaction count of one load
+  uint8_t ndim;        // 5 when the sweep runs in TMA form, else 0
+  uint8_t store;       // plain write-backs go out as TMA stores
+  uint8_t start[5];    // free dimension: first index bit of its run
+  uint32_t mask[5];    // free dimension: 2^len - 1 (0: a tile dimension)
+  // host side: the maps' shape (words of 8 bytes), encoded at launch
+  cuuint64_t gdim[5];
+  cuuint64_t gstride[4];
+  cuuint32_t box[5];
+};
+// a tile load that has not arrived after this long abandons the sweep
+constexpr uint64_t kTmaWaitNs = 2000000000ull;
 
 // ---------------------------------------------------------------- limits
 // 31 qubits at most, the reference's limit (execution.py:23-25): the
@@ -230,6 +257,13 @@ int check_tile_fault(mq_state* h);
 // Looks up the driver's tensor-map encoder once per process (state creation
 // calls it, so that no lookup happens inside a stream capture).
 void prepare_tile_maps();
+// TMA tiles (mq_tile.cu): on unless MQ_TMA=0; the shape of a sweep's tiles
+// (false when the TMA form cannot describe it); the two maps of a launch.
+bool tma_enabled();
+bool plan_tma(int n, size_t amp_bytes, const std::vector<int>& tile_bits, TmaDesc& D);
+int encode_tile_maps(TmaDesc& D, void* src, void* dst);
+// The adjoint sweeps' abandoned-work flag, read and cleared (mq_adjoint.cu).
+int take_adj_fault(mq_state* h, bool* fault);
 
 // ------------------------------------------------------------ launchers
 // Tile sweeps: U(2) layer and QFT (mq_tile.cu)

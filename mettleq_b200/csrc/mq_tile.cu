@@ -85,30 +85,6 @@ struct __align__(16) PhaseDesc {
 static_assert(offsetof(PhaseDesc, uf) % 16 == 0, "matrix rows must be 16-byte aligned");
 static_assert(sizeof(PhaseDesc) % 16 == 0, "PhaseDesc array stride must keep rows aligned");
 
-// TMA form of a sweep's tile movement.  The state is viewed as a tensor of
-// 8-byte words (complex64: one amplitude; complex128: its real or imaginary
-// part, word bit 0) whose dimensions are runs of index bits in ascending
-// order: dimension 0 is word bits [0, 4) (128 bytes), then alternately runs
-// of tile bits (box = the whole run, split at 8 bits) and runs of free bits
-// (box 1; coordinate = the tile base's bits there).  A tile is then one box,
-// and the tensor map's 128-byte swizzle puts 16-byte chunk j of 128-byte
-// row r at chunk j ^ (r & 7): the chunk layout the register phases already
-// use (amp_slot), so the phases read TMA-loaded tiles unchanged.
-struct alignas(64) TmaDesc {
-  CUtensorMap src;     // over the buffer the sweep reads
-  CUtensorMap dst;     // over the buffer it writes (the same one in place)
-  uint32_t bytes;      // one tile: the transaction count of one load
-  uint8_t ndim;        // 5 when the sweep runs in TMA form, else 0
-  uint8_t store;       // plain write-backs go out as TMA stores
-  uint8_t start[5];    // free dimension: first index bit of its run
-  uint32_t mask[5];    // free dimension: 2^len - 1 (0: a tile dimension)
-  // host side: the maps' shape (words of 8 bytes), encoded at launch
-  cuuint64_t gdim[5];
-  cuuint64_t gstride[4];
-  cuuint32_t box[5];
-};
-// a tile load that has not arrived after this long abandons the sweep
-constexpr uint64_t kTmaWaitNs = 2000000000ull;
 // set when a sweep was abandoned (read and cleared by mq_sync)
 __device__ unsigned int g_tile_fault;
 
@@ -974,7 +950,6 @@ static int tile13_lt() { return env_int("MQ_TILE13_LT", 8, 8, 9); }
 // per-thread copies that paid (fused config layer at 30 qubits 15.6 -> 15.5
 // ms); with TMA tiles the 12-bit tile and its second buffer win (30 qubits
 // 14.07 -> 13.76 ms), so the default follows the tile movement.
-static bool tma_enabled();
 static bool euler_hi13() { return env_int("MQ_EULER_HI13", tma_enabled() ? 0 : 1, 0, 1) == 1; }
 // U(2) layers without diagonal terms through the Euler split as well.
 static bool euler_plain() { return env_int("MQ_EULER_PLAIN", 1, 0, 1) == 1; }
@@ -1036,7 +1011,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 void prepare_tile_maps() { (void)tensor_map_encoder(); }
 
 // The tensor maps of a TMA sweep over the buffers it reads and writes.
-static int encode_tile_maps(TmaDesc& D, void* src, void* dst) {
+int encode_tile_maps(TmaDesc& D, void* src, void* dst) {
   auto enc = tensor_map_encoder();
   if (!enc) return fail(MQ_EDEVICE, "cuTensorMapEncodeTiled is not available from the CUDA driver");
   const cuuint32_t estride[5] = {1, 1, 1, 1, 1};
@@ -1265,13 +1240,16 @@ static void fill_epi(EpiDesc& D, const EpiPlan& e, int m, int n) {
 }
 
 // Tile movement by TMA (MQ_TMA=0: per-thread asynchronous copies throughout).
-static bool tma_enabled() { return env_int("MQ_TMA", 1, 0, 1) == 1; }
+bool tma_enabled() { return env_int("MQ_TMA", 1, 0, 1) == 1; }
 
 int check_tile_fault(mq_state* h) {
   unsigned int v = 0;
   MQ_CUDA(cudaMemcpyFromSymbolAsync(&v, g_tile_fault, sizeof(v), 0, cudaMemcpyDeviceToHost, h->stream));
   MQ_CUDA(cudaStreamSynchronize(h->stream));
-  if (!v) return MQ_OK;
+  bool adj = false;
+  int rc = take_adj_fault(h, &adj);
+  if (rc) return rc;
+  if (!v && !adj) return MQ_OK;
   const unsigned int zero = 0;
   MQ_CUDA(cudaMemcpyToSymbolAsync(g_tile_fault, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, h->stream));
   MQ_CUDA(cudaStreamSynchronize(h->stream));
@@ -1281,7 +1259,7 @@ int check_tile_fault(mq_state* h) {
 // The TMA shape of a sweep's tiles (see TmaDesc): false when it needs more
 // than five dimensions or the tile lacks the low 128 bytes of its rows.
 // Dimensions of size 1 above the state pad the maps to five.
-static bool plan_tma(int n, size_t amp_bytes, const std::vector<int>& tile_bits, TmaDesc& D) {
+bool plan_tma(int n, size_t amp_bytes, const std::vector<int>& tile_bits, TmaDesc& D) {
   const int s = amp_bytes == 16 ? 1 : 0;  // word bits below the amplitude bits (real / imaginary part)
   const int nw = n + s;
   if (nw < 4) return false;
