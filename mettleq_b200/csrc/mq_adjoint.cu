@@ -355,20 +355,35 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
 }
 
 // lam_x = d(x) psi_x with d(x) = sum_w c_w (-1)^popcount(x & z_w).
+// Words whose support lies within 8 consecutive index bits are summed on the
+// host into window tables: tab[k][v] = sum over the window's words of
+// c_w (-1)^popcount(v & (z_w >> shift_k)), so d(x) = base + sum_k
+// tab[k][(x >> shift_k) & 255] + the remaining (wider) words one by one.  An
+// Ising chain's ZZ terms then cost one shared-memory read per window instead
+// of a popcount per term, and the pass runs at memory speed.
 constexpr int kHZWords = 64;
+constexpr int kHTab = 8;  // window tables of 256 entries
 struct HDiagParams {
   uint32_t dim;
-  int32_t nz;
+  int32_t nz;          // words evaluated one by one
   uint32_t z[kHZWords];
   double c[kHZWords];
+  int32_t ntab;        // window tables
+  uint8_t shift[kHTab];
+  double base;         // words without a Z factor
+  double tab[kHTab][256];
 };
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_hdiag(const V2<R>* __restrict__ psi, V2<R>* __restrict__ lam,
                                                const __grid_constant__ HDiagParams P) {
+  __shared__ R tab[kHTab * 256];
+  for (int j = threadIdx.x; j < P.ntab * 256; j += blockDim.x) tab[j] = (R)P.tab[j >> 8][j & 255];
+  __syncthreads();
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < P.dim; i += stride) {
-    R d = 0;
+    R d = (R)P.base;
+    for (int k = 0; k < P.ntab; ++k) d += tab[k * 256 + ((i >> P.shift[k]) & 255u)];
     for (int w = 0; w < P.nz; ++w) d += (__popc(i & P.z[w]) & 1) ? -(R)P.c[w] : (R)P.c[w];
     const V2<R> v = psi[i];
     lam[i] = mk<R>(d * v.x, d * v.y);
@@ -700,11 +715,38 @@ int apply_hamiltonian(mq_state* psi, mq_state* lam, int n_z, const uint64_t* zma
   HDiagParams H;
   std::memset(&H, 0, sizeof(H));
   H.dim = (uint32_t)psi->dim();
-  H.nz = n_z;
-  for (int w = 0; w < n_z; ++w) {
+  for (int w = 0; w < n_z; ++w)
     if (zmasks[w] & ~lim) return fail(MQ_EINVAL, "Pauli mask outside the register");
-    H.z[w] = (uint32_t)zmasks[w];
-    H.c[w] = zcoef[w];
+  // window tables: from the lowest remaining word, every word whose support
+  // fits in the 8 bits [lo, lo + 8) joins the table of that window
+  std::vector<bool> done(n_z, false);
+  for (int w = 0; w < n_z; ++w)
+    if (zmasks[w] == 0) { H.base += zcoef[w]; done[w] = true; }
+  auto lowbit = [](uint64_t z) { return __builtin_ctzll(z); };
+  auto highbit = [](uint64_t z) { return 63 - __builtin_clzll(z); };
+  while (H.ntab < kHTab) {
+    int first = -1;
+    for (int w = 0; w < n_z; ++w)
+      if (!done[w] && highbit(zmasks[w]) - lowbit(zmasks[w]) < 8 &&
+          (first < 0 || lowbit(zmasks[w]) < lowbit(zmasks[first])))
+        first = w;
+    if (first < 0) break;
+    const int lo = lowbit(zmasks[first]);
+    double* t = H.tab[H.ntab];
+    for (int w = 0; w < n_z; ++w) {
+      if (done[w] || lowbit(zmasks[w]) < lo || highbit(zmasks[w]) >= lo + 8) continue;
+      const uint32_t zl = (uint32_t)(zmasks[w] >> lo);
+      for (int v = 0; v < 256; ++v) t[v] += (__builtin_popcount((uint32_t)v & zl) & 1) ? -zcoef[w] : zcoef[w];
+      done[w] = true;
+    }
+    H.shift[H.ntab] = (uint8_t)lo;
+    ++H.ntab;
+  }
+  for (int w = 0; w < n_z; ++w) {
+    if (done[w]) continue;
+    H.z[H.nz] = (uint32_t)zmasks[w];
+    H.c[H.nz] = zcoef[w];
+    ++H.nz;
   }
   const uint32_t dim = (uint32_t)psi->dim();
   const uint32_t grid = (uint32_t)std::min<uint64_t>((dim + 255) / 256, (uint64_t)psi->num_sms * 8);

@@ -191,6 +191,41 @@ def test_pauli_sum_energy_and_lambda():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("seed", [1, 2])
+def test_pauli_sum_window_tables_and_wide_words(seed):
+    """lam = H psi for random Z words of every width (one to all qubits), a
+    constant word and a chain: the words within 8 index bits go through the
+    window tables, the wider ones one by one."""
+    from mettleq_b200.adjoint import AdjointEngine
+    n = 16
+    rng = np.random.default_rng(seed)
+    words = [((i, i + 1), float(rng.uniform(-1, 1))) for i in range(n - 1)]
+    for k in (1, 2, 3, 5, 9, 16):
+        for _ in range(3):
+            words.append((tuple(sorted(int(q) for q in rng.choice(n, k, replace=False))), float(rng.uniform(-1, 1))))
+    words.append(((), 0.25))
+    H = PauliSum(n, words, None)
+    eng = AdjointEngine(LayeredAnsatz(n, 1), H, dtype="complex128")
+    try:
+        vec = rand_state(n, seed, np.complex128)
+        eng.psi.set(vec)
+        e = eng._pauli_sum()
+        lam = eng.lam.get()
+    finally:
+        eng.close()
+    idx = np.arange(1 << n)
+    d = np.zeros(1 << n)
+    for w, c in words:
+        z = 0
+        for q in w:
+            z |= 1 << (n - 1 - q)
+        par = np.array([bin(int(x)).count("1") & 1 for x in (idx & z)])
+        d += c * (1 - 2 * par)
+    assert np.max(np.abs(lam - d * vec)) < 1e-12
+    assert abs(e - float(np.real(np.vdot(vec, d * vec)))) < 1e-12
+
+
+@pytest.mark.gpu
 def test_host_and_device_gradient_readback_agree(monkeypatch):
     """mq_adjoint_layer (host gradients, one wait per layer) and
     mq_adjoint_layer_async (device gradients, one read at the end) give the
