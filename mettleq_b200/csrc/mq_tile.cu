@@ -819,6 +819,42 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
         }
       }
     }
+    if constexpr (STORE_EPI && TMA && CB == 1) {
+      if (P.tma.store == 2) {
+        // permutation keeping index bit 0: output chunk c = tid + k*NT is the
+        // input pair at l0 = cl ^ A(c << 1) (swapped when l0 is odd).  Every
+        // thread reads its chunks, the barrier ends all reads of the tile,
+        // the chunks go to their output slots, and the tile leaves as one
+        // TMA store to output tile `tile`
+        float4 v[CPT];
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+          const uint32_t l0 = cl_in ^ epi_ak[k];
+          const float4 w = *reinterpret_cast<const float4*>(cur + amp_slot<R>(l0 & ~1u));
+          v[k] = (l0 & 1u) ? make_float4(w.z, w.w, w.x, w.y) : w;
+        }
+        __syncthreads();
+        float4* c4w = reinterpret_cast<float4*>(cur);
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) c4w[slot(k)] = v[k];
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+          int32_t c[5];
+          tma_coords(tile << M, c);
+          tma_store_5d(&P.tma.dst, c, smem_u32(cur));
+          bulk_commit();
+          if constexpr (NBUF == 1) {
+            const uint32_t next = tile + gridDim.x;
+            if (next < P.n_tiles) {
+              bulk_wait_read();
+              tma_load_tile(next, 0);
+            }
+          }
+        }
+        continue;
+      }
+    }
     if constexpr (STORE_EPI) {
       if (P.epi.perm || P.epi.diag) {
         epilogue_store<R, M, LT, CPT>(P.epi, cur, ecols, elut, dst, tile << M, base, cl_in, tid, epi_ak);
@@ -1241,6 +1277,9 @@ static void fill_epi(EpiDesc& D, const EpiPlan& e, int m, int n) {
 
 // Tile movement by TMA (MQ_TMA=0: per-thread asynchronous copies throughout).
 bool tma_enabled() { return env_int("MQ_TMA", 1, 0, 1) == 1; }
+// The fused layer's permuted write-back gathered in shared memory and
+// TMA-stored (1) or stored per thread (0).
+static bool tma_perm_store() { return env_int("MQ_TMA_PERM_STORE", 1, 0, 1) == 1; }
 
 int check_tile_fault(mq_state* h) {
   unsigned int v = 0;
@@ -1328,11 +1367,16 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
   P.n_ops = (uint8_t)sw.ops.size();
   for (int k = 0; k < m; ++k) P.tile_bit[k] = (uint8_t)sw.tile_bits[k];
   make_base_runs(P.runs, h->n, P.tile_bit, m);
-  // TMA form for tiles of 10 bits and more whose shape it can describe;
-  // the write-back is a TMA store unless it scatters (permutation) or
-  // multiplies per amplitude (window diagonal)
-  if (tma_enabled() && m >= 10 && !sw.phases.empty() && plan_tma(h->n, h->amp_bytes(), sw.tile_bits, P.tma))
-    P.tma.store = (epi && (epi->perm || epi->diag)) ? 0 : 1;
+  // TMA form for tiles of 10 bits and more whose shape it can describe.
+  // Write-back: a TMA store of the tile in place (1); for a permutation that
+  // keeps index bit 0 (complex64, no window diagonal), the output tile is
+  // gathered in shared memory and then TMA-stored (2); otherwise per-thread
+  // stores (0)
+  if (tma_enabled() && m >= 10 && !sw.phases.empty() && plan_tma(h->n, h->amp_bytes(), sw.tile_bits, P.tma)) {
+    if (!epi || (!epi->perm && !epi->diag)) P.tma.store = 1;
+    else if (epi->perm && !epi->diag && epi->cols[0] == 1u && h->dtype == MQ_C64 && tma_perm_store()) P.tma.store = 2;
+    else P.tma.store = 0;
+  }
   // chunk-index bits above the thread bits: contiguous global bits?
   {
     const int cb = h->dtype == MQ_C64 ? 1 : 0;
