@@ -29,6 +29,25 @@ template <typename T> __device__ __forceinline__ T cmulc(T a, T b) {  // a * con
   T r; r.x = a.x * b.x + a.y * b.y; r.y = a.y * b.x - a.x * b.y; return r;
 }
 template <typename T, typename R> __device__ __forceinline__ T cscale(T a, R s) { a.x *= s; a.y *= s; return a; }
+// x + t y for a real t
+template <typename T, typename R> __device__ __forceinline__ T caxpy(R t, T y, T x) {
+  x.x = fma(t, y.x, x.x); x.y = fma(t, y.y, x.y); return x;
+}
+// t y - x for a real t
+template <typename T, typename R> __device__ __forceinline__ T caxmy(R t, T y, T x) {
+  x.x = fma(t, y.x, -x.x); x.y = fma(t, y.y, -x.y); return x;
+}
+// complex64 on the paired FP32 instructions of sm_100 (FADD2 / FMUL2 /
+// FFMA2): one instruction where the components take the same operation.
+// Each lane rounds like the scalar instruction, so the results are the bits
+// of the scalar forms above (a - b as a + (-1) b: the product is exact).
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+__device__ __forceinline__ float2 caxpy(float t, float2 y, float2 x) { return __ffma2_rn(make_float2(t, t), y, x); }
+__device__ __forceinline__ float2 caxmy(float t, float2 y, float2 x) {
+  return __ffma2_rn(make_float2(t, t), y, make_float2(-x.x, -x.y));
+}
 
 // ---------------------------------------------------------------- async copies
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

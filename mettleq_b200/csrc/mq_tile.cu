@@ -229,20 +229,16 @@ __device__ __forceinline__ void apply_u2(V2<R> (&a)[1 << LR], const PhaseDesc& D
       for (int r = 0; r < NR; ++r) {
         if (r & (1 << K)) continue;
         const T x0 = a[r], x1 = a[r | (1 << K)];
-        a[r].x = fma(t, x0.x, -x1.x);
-        a[r].y = fma(t, x0.y, -x1.y);
-        a[r | (1 << K)].x = fma(t, x1.x, x0.x);
-        a[r | (1 << K)].y = fma(t, x1.y, x0.y);
+        a[r] = caxmy(t, x0, x1);
+        a[r | (1 << K)] = caxpy(t, x1, x0);
       }
     } else {
 #pragma unroll
       for (int r = 0; r < NR; ++r) {
         if (r & (1 << K)) continue;
         const T x0 = a[r], x1 = a[r | (1 << K)];
-        a[r].x = fma(-t, x1.x, x0.x);
-        a[r].y = fma(-t, x1.y, x0.y);
-        a[r | (1 << K)].x = fma(t, x0.x, x1.x);
-        a[r | (1 << K)].y = fma(t, x0.y, x1.y);
+        a[r] = caxpy(-t, x1, x0);
+        a[r | (1 << K)] = caxpy(t, x0, x1);
       }
     }
     return;
@@ -254,10 +250,8 @@ __device__ __forceinline__ void apply_u2(V2<R> (&a)[1 << LR], const PhaseDesc& D
     for (int r = 0; r < NR; ++r) {
       if (r & (1 << K)) continue;
       const T x0 = a[r], x1 = a[r | (1 << K)];
-      a[r].x = fma(c00, x0.x, c01 * x1.x);
-      a[r].y = fma(c00, x0.y, c01 * x1.y);
-      a[r | (1 << K)].x = fma(c10, x0.x, c11 * x1.x);
-      a[r | (1 << K)].y = fma(c10, x0.y, c11 * x1.y);
+      a[r] = caxpy(c00, x0, cscale(x1, c01));
+      a[r | (1 << K)] = caxpy(c10, x0, cscale(x1, c11));
     }
     return;
   }
@@ -784,10 +778,7 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
           // is applied here instead of in the write-back (the same product)
           if (ph == P.n_phases - 1) {
 #pragma unroll
-            for (int r = 0; r < NR; ++r) {
-              a[r].x *= (R)P.scale;
-              a[r].y *= (R)P.scale;
-            }
+            for (int r = 0; r < NR; ++r) a[r] = cscale(a[r], (R)P.scale);
           }
         }
         if (pair) {
