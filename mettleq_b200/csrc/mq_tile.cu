@@ -371,6 +371,19 @@ __device__ __forceinline__ V2<R> epi_phase(const EpiDesc& D, const V2<R>* lut, u
   return f;
 }
 
+constexpr int ilog2_c(int x) { return x <= 1 ? 0 : 1 + ilog2_c(x >> 1); }
+
+// A applied to the chunk-index bits of k*NT (chunk c = tid + k*NT, amplitude
+// c << CB): the XOR of the permutation columns of k's set bits
+template <int LT, int LCH, int CB>
+__device__ __forceinline__ uint32_t chunk_cols(int k, const uint32_t* cols) {
+  uint32_t a = 0;
+#pragma unroll
+  for (int b = 0; b < LCH; ++b)
+    if ((k >> b) & 1) a ^= cols[CB + LT + b];
+  return a;
+}
+
 // MODE 2 write-back: output chunk c = tid + k*NT of output tile bo holds
 // amplitudes y = c << CB (and y | 1 for complex64); their values are the
 // processed input amplitudes l = cl ^ A y (identity without a permutation)
@@ -378,10 +391,11 @@ __device__ __forceinline__ V2<R> epi_phase(const EpiDesc& D, const V2<R>* lut, u
 template <typename R, int M, int LT, int CPT>
 __device__ __forceinline__ void epilogue_store(const EpiDesc& D, const V2<R>* cur, const uint32_t* cols,
                                                const V2<R>* lut, V2<R>* dst, uint32_t bo, uint32_t ib, uint32_t cl,
-                                               int tid, const uint32_t (&ak)[CPT]) {
+                                               int tid, uint32_t at) {
   using T = V2<R>;
   constexpr int NT = 1 << LT;
   constexpr int CB = sizeof(T) == 8 ? 1 : 0;
+  constexpr int LCH = ilog2_c(CPT);
   const bool perm = D.perm, diag = D.diag;
   T hc = mk<R>(1, 0);
   if (diag) {
@@ -396,7 +410,7 @@ __device__ __forceinline__ void epilogue_store(const EpiDesc& D, const V2<R>* cu
 #pragma unroll
       for (int k = 0; k < CPT; ++k) {
         const uint32_t y = ((uint32_t)tid + (uint32_t)(k * NT)) << 1;
-        const uint32_t l0 = cl ^ ak[k];
+        const uint32_t l0 = cl ^ at ^ chunk_cols<LT, LCH, CB>(k, cols);
         const float4 v = *reinterpret_cast<const float4*>(cur + amp_slot<R>(l0 & ~1u));
         *reinterpret_cast<float4*>(dst + (bo | y)) = (l0 & 1u) ? make_float4(v.z, v.w, v.x, v.y) : v;
       }
@@ -406,7 +420,7 @@ __device__ __forceinline__ void epilogue_store(const EpiDesc& D, const V2<R>* cu
 #pragma unroll
   for (int k = 0; k < CPT; ++k) {
     const uint32_t y = ((uint32_t)tid + (uint32_t)(k * NT)) << CB;
-    const uint32_t l0 = perm ? (cl ^ ak[k]) : y;
+    const uint32_t l0 = perm ? (cl ^ at ^ chunk_cols<LT, LCH, CB>(k, cols)) : y;
     T v0 = cur[amp_slot<R>(l0)];
     if (diag) v0 = cmul(v0, epi_phase<R>(D, lut, ib | l0, hc));
     if constexpr (CB == 1) {
@@ -551,25 +565,16 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   __syncthreads();
 
   if constexpr (QFT) tw = g_qft_twiddles;
-  // MODE 2 with a permutation: A applied to the low offsets of this thread's
-  // output chunks (c = tid + k*NT -> amplitude c << CB), computed once
-  uint32_t epi_ak[STORE_EPI ? CPT : 1];
-#pragma unroll
-  for (int k = 0; k < (STORE_EPI ? CPT : 1); ++k) epi_ak[k] = 0;
+  // MODE 2 with a permutation: A applied to the thread part of this
+  // thread's output chunks (c = tid + k*NT -> amplitude c << CB), computed
+  // once; the part of k*NT comes from the columns at the write-back (one
+  // register held through the sweep instead of CPT)
+  uint32_t epi_at = 0;
   if constexpr (STORE_EPI) {
     if (P.epi.perm) {
-      uint32_t at = 0;
 #pragma unroll
       for (int b = 0; b < LT; ++b)
-        if ((tid >> b) & 1) at ^= ecols[CB + b];
-#pragma unroll
-      for (int k = 0; k < CPT; ++k) {
-        uint32_t a = at;
-#pragma unroll
-        for (int b = 0; b < LCH; ++b)
-          if ((k >> b) & 1) a ^= ecols[CB + LT + b];
-        epi_ak[k] = a;
-      }
+        if ((tid >> b) & 1) epi_at ^= ecols[CB + b];
     }
   }
 
@@ -820,7 +825,7 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
         float4 v[CPT];
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-          const uint32_t l0 = cl_in ^ epi_ak[k];
+          const uint32_t l0 = cl_in ^ epi_at ^ chunk_cols<LT, LCH, CB>(k, ecols);
           const float4 w = *reinterpret_cast<const float4*>(cur + amp_slot<R>(l0 & ~1u));
           v[k] = (l0 & 1u) ? make_float4(w.z, w.w, w.x, w.y) : w;
         }
@@ -848,7 +853,7 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
     }
     if constexpr (STORE_EPI) {
       if (P.epi.perm || P.epi.diag) {
-        epilogue_store<R, M, LT, CPT>(P.epi, cur, ecols, elut, dst, tile << M, base, cl_in, tid, epi_ak);
+        epilogue_store<R, M, LT, CPT>(P.epi, cur, ecols, elut, dst, tile << M, base, cl_in, tid, epi_at);
         if constexpr (TMA && NBUF == 1) {
           __syncthreads();
           const uint32_t next = tile + gridDim.x;
