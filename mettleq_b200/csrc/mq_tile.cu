@@ -99,6 +99,10 @@ struct TileParams {
   double scale;
   uint8_t ph_op[kMaxPhases + 2];     // QFT: ops of phase p are [ph_op[p], ph_op[p+1])
   uint8_t qchain[kMaxPhases];        // QFT: 1 + the largest width when the phase's stages chain (else 0)
+  // QFT: 1 when a chained phase holds four stages, one per register slot, in
+  // the order of their direction (slots 3..0 forward, 0..3 inverse): its
+  // register factors are then compile-time constants (apply_qft_chain4)
+  uint8_t qfull[kMaxPhases];
   // U(2) matrices read from device memory at launch (mats_dev[8 q ..]):
   // slot k of phase p takes row mat_q[p][k] - 1 (0 = the matrix in ph)
   int16_t mat_q[kMaxPhases][5];
@@ -342,6 +346,91 @@ template <typename R, int LR>
 __device__ __forceinline__ void apply_qft_op(V2<R> (&a)[1 << LR], const TileOp& op, V2<R> tg, const V2<R>* treg) {
   if (op.kind == OP_QFT_FWD) apply_qft_dir<R, LR, true>(a, op, tg, treg);
   else apply_qft_dir<R, LR, false>(a, op, tg, treg);
+}
+
+// A phase of four chained QFT stages, one per register slot of a 16-amplitude
+// group, on consecutive ladder bits.  The stage on slot K has width
+// wmax - (3 - K); its pair (r, r | 2^K) takes the factor
+//   e^{i pi Lg / 2^{width}} e^{i pi rho / 2^K},  rho = r mod 2^K,
+// the first the group factor p^(2^(3-K)) (p the top stage's), the second a
+// compile-time constant: a multiple of pi/8, formed from the group factor by
+// a quarter turn (free), the pi/4 rotation (two adds, two products) or one
+// complex product with cos/sin(pi/8).
+template <typename R, int K, int RHO>
+__device__ __forceinline__ V2<R> qft_wk(V2<R> tg, const V2<R>* wk) {
+  constexpr int N = 1 << K;       // angle pi RHO / N, RHO < N
+  constexpr int E = RHO * (8 / N);  // the same angle in units of pi/8
+  constexpr R kC8 = (R)0.92387953251128675613, kS8 = (R)0.38268343236508977173;
+  constexpr R kH = (R)0.70710678118654752440;
+  if constexpr (E == 0) {
+    return tg;
+  } else if constexpr (E >= 4) {  // a quarter turn after the factor of angle - pi/2
+    const V2<R> b = wk[RHO - N / 2];
+    return mk<R>(-b.y, b.x);
+  } else if constexpr (E == 2) {
+    return mk<R>((tg.x - tg.y) * kH, (tg.x + tg.y) * kH);
+  } else if constexpr (E == 1) {
+    return cmul(tg, mk<R>(kC8, kS8));
+  } else {
+    return cmul(tg, mk<R>(kS8, kC8));
+  }
+}
+
+template <typename R, int K, bool FWD>
+__device__ __forceinline__ void qft_slot(V2<R> (&a)[16], V2<R> tg) {
+  using T = V2<R>;
+  constexpr int NW = 1 << K;
+  T wk[NW];
+  wk[0] = tg;
+  if constexpr (NW > 1) wk[1] = qft_wk<R, K, 1>(tg, wk);
+  if constexpr (NW > 2) {
+    wk[2] = qft_wk<R, K, 2>(tg, wk);
+    wk[3] = qft_wk<R, K, 3>(tg, wk);
+  }
+  if constexpr (NW > 4) {
+    wk[4] = qft_wk<R, K, 4>(tg, wk);
+    wk[5] = qft_wk<R, K, 5>(tg, wk);
+    wk[6] = qft_wk<R, K, 6>(tg, wk);
+    wk[7] = qft_wk<R, K, 7>(tg, wk);
+  }
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    if (r & (1 << K)) continue;
+    const int r1 = r | (1 << K);
+    const T w = wk[r & (NW - 1)];
+    T x0 = a[r], x1 = a[r1];
+    if constexpr (FWD) {
+      a[r] = cadd(x0, x1);
+      a[r1] = cmul(csub(x0, x1), w);
+    } else {
+      x1 = cmulc(x1, w);
+      a[r] = cadd(x0, x1);
+      a[r1] = csub(x0, x1);
+    }
+  }
+}
+
+// p: the group factor of the top stage (slot 3, width wmax); slot K takes
+// p^(2^(3-K)).  Forward stages run from slot 3 down, inverse ones from slot
+// 0 up (conjugate factors), as apply_qft does one stage at a time.
+template <typename R, bool FWD>
+__device__ __forceinline__ void apply_qft_chain4(V2<R> (&a)[16], V2<R> p) {
+  using T = V2<R>;
+  T pw[4];
+  pw[0] = p;
+#pragma unroll
+  for (int d = 1; d < 4; ++d) pw[d] = cmul(pw[d - 1], pw[d - 1]);
+  if constexpr (FWD) {
+    qft_slot<R, 3, true>(a, pw[0]);
+    qft_slot<R, 2, true>(a, pw[1]);
+    qft_slot<R, 1, true>(a, pw[2]);
+    qft_slot<R, 0, true>(a, pw[3]);
+  } else {
+    qft_slot<R, 0, false>(a, pw[3]);
+    qft_slot<R, 1, false>(a, pw[2]);
+    qft_slot<R, 2, false>(a, pw[1]);
+    qft_slot<R, 3, false>(a, pw[0]);
+  }
 }
 
 // The group factor of a stage from the twiddle tables (Lg = 0 reads entry 0
@@ -743,15 +832,25 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
               const uint32_t mask = (wmax >= 32) ? 0xffffffffu : ((1u << wmax) - 1u);
               pw[0] = Twiddle<R>::get(tw, (gq >> P.ops[o0].lad_shift) & mask, wmax);
             }
+            bool done = false;
+            if constexpr (LR == 4) {
+              if (P.qfull[ph]) {
+                if (P.ops[o0].kind == OP_QFT_FWD) apply_qft_chain4<R, true>(a, pw[0]);
+                else apply_qft_chain4<R, false>(a, pw[0]);
+                done = true;
+              }
+            }
+            if (!done) {
 #pragma unroll
-            for (int d = 1; d < LR; ++d) pw[d] = cmul(pw[d - 1], pw[d - 1]);
-            for (int o = o0; o < o1; ++o) {
-              const int d = wmax - P.ops[o].width;
-              T tg = pw[0];
+              for (int d = 1; d < LR; ++d) pw[d] = cmul(pw[d - 1], pw[d - 1]);
+              for (int o = o0; o < o1; ++o) {
+                const int d = wmax - P.ops[o].width;
+                T tg = pw[0];
 #pragma unroll
-              for (int e = 1; e < LR; ++e)
-                if (d == e) tg = pw[e];
-              apply_qft_op<R, LR>(a, P.ops[o], tg, qreg + 32 * o);
+                for (int e = 1; e < LR; ++e)
+                  if (d == e) tg = pw[e];
+                apply_qft_op<R, LR>(a, P.ops[o], tg, qreg + 32 * o);
+              }
             }
           } else {
             for (int o = o0; o < o1; ++o)
@@ -1276,6 +1375,9 @@ bool tma_enabled() { return env_int("MQ_TMA", 1, 0, 1) == 1; }
 // The fused layer's permuted write-back gathered in shared memory and
 // TMA-stored (1) or stored per thread (0).
 static bool tma_perm_store() { return env_int("MQ_TMA_PERM_STORE", 1, 0, 1) == 1; }
+// QFT phases of four chained stages on compile-time register factors (1) or
+// through the per-stage path (0).
+static bool qft_full_phases() { return env_int("MQ_QFT_FULL", 1, 0, 1) == 1; }
 
 int check_tile_fault(mq_state* h) {
   unsigned int v = 0;
@@ -1432,6 +1534,18 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
         gmax = std::max(gmax, g);
       }
       if (chain && gmax - gmin == o1 - o0 - 1 && wmax <= 31) P.qchain[p] = (uint8_t)(wmax + 1);
+      // four stages on the four register slots of a 16-amplitude phase,
+      // every slot's stage in the order of the direction
+      if (P.qchain[p] && lr == 4 && o1 - o0 == 4 && wmax >= 3 && qft_full_phases()) {
+        const bool fwd = P.ops[o0].kind == OP_QFT_FWD;
+        bool full = true;
+        for (int i = 0; i < 4; ++i) {
+          const TileOp& op = P.ops[o0 + i];
+          full = full && op.kind == P.ops[o0].kind && op.rk == (fwd ? 3 - i : i) &&
+                 op.width == (fwd ? wmax - i : wmax - 3 + i);
+        }
+        P.qfull[p] = full ? 1 : 0;
+      }
     }
   } else {
     for (size_t o = 0; o < sw.ops.size(); ++o) {
