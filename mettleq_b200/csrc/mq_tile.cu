@@ -99,9 +99,10 @@ struct TileParams {
   double scale;
   uint8_t ph_op[kMaxPhases + 2];     // QFT: ops of phase p are [ph_op[p], ph_op[p+1])
   uint8_t qchain[kMaxPhases];        // QFT: 1 + the largest width when the phase's stages chain (else 0)
-  // QFT: 1 when a chained phase holds four stages, one per register slot, in
-  // the order of their direction (slots 3..0 forward, 0..3 inverse): its
-  // register factors are then compile-time constants (apply_qft_chain4)
+  // QFT: ns (3 or 4) when a chained phase holds ns stages on register slots
+  // 0 .. ns-1 in the order of their direction (top slot first forward, slot
+  // 0 first inverse): its register factors are then compile-time constants
+  // (apply_qft_chain); 0 otherwise
   uint8_t qfull[kMaxPhases];
   // U(2) matrices read from device memory at launch (mats_dev[8 q ..]):
   // slot k of phase p takes row mat_q[p][k] - 1 (0 = the matrix in ph)
@@ -348,11 +349,11 @@ __device__ __forceinline__ void apply_qft_op(V2<R> (&a)[1 << LR], const TileOp& 
   else apply_qft_dir<R, LR, false>(a, op, tg, treg);
 }
 
-// A phase of four chained QFT stages, one per register slot of a 16-amplitude
+// A phase of chained QFT stages, one per register slot of a 16-amplitude
 // group, on consecutive ladder bits.  The stage on slot K has width
-// wmax - (3 - K); its pair (r, r | 2^K) takes the factor
+// wmax - (top - K); its pair (r, r | 2^K) takes the factor
 //   e^{i pi Lg / 2^{width}} e^{i pi rho / 2^K},  rho = r mod 2^K,
-// the first the group factor p^(2^(3-K)) (p the top stage's), the second a
+// the first the group factor p^(2^(top-K)) (p the top stage's), the second a
 // compile-time constant: a multiple of pi/8, formed from the group factor by
 // a quarter turn (free), the pi/4 rotation (two adds, two products) or one
 // complex product with cos/sin(pi/8).
@@ -410,26 +411,28 @@ __device__ __forceinline__ void qft_slot(V2<R> (&a)[16], V2<R> tg) {
   }
 }
 
-// p: the group factor of the top stage (slot 3, width wmax); slot K takes
-// p^(2^(3-K)).  Forward stages run from slot 3 down, inverse ones from slot
-// 0 up (conjugate factors), as apply_qft does one stage at a time.
-template <typename R, bool FWD>
-__device__ __forceinline__ void apply_qft_chain4(V2<R> (&a)[16], V2<R> p) {
+// NS chained stages (3 or 4) on register slots 0 .. NS-1 (a fourth slot
+// above them carries no stage).  p: the group factor of the top stage (slot
+// NS-1, width wmax); slot K takes p^(2^(NS-1-K)).  Forward stages run from
+// the top slot down, inverse ones from slot 0 up (conjugate factors), as
+// apply_qft does one stage at a time.
+template <typename R, bool FWD, int NS>
+__device__ __forceinline__ void apply_qft_chain(V2<R> (&a)[16], V2<R> p) {
   using T = V2<R>;
-  T pw[4];
+  T pw[NS];
   pw[0] = p;
 #pragma unroll
-  for (int d = 1; d < 4; ++d) pw[d] = cmul(pw[d - 1], pw[d - 1]);
+  for (int d = 1; d < NS; ++d) pw[d] = cmul(pw[d - 1], pw[d - 1]);
   if constexpr (FWD) {
-    qft_slot<R, 3, true>(a, pw[0]);
-    qft_slot<R, 2, true>(a, pw[1]);
-    qft_slot<R, 1, true>(a, pw[2]);
-    qft_slot<R, 0, true>(a, pw[3]);
+    if constexpr (NS == 4) qft_slot<R, 3, true>(a, pw[NS - 4]);
+    qft_slot<R, 2, true>(a, pw[NS - 3]);
+    qft_slot<R, 1, true>(a, pw[NS - 2]);
+    qft_slot<R, 0, true>(a, pw[NS - 1]);
   } else {
-    qft_slot<R, 0, false>(a, pw[3]);
-    qft_slot<R, 1, false>(a, pw[2]);
-    qft_slot<R, 2, false>(a, pw[1]);
-    qft_slot<R, 3, false>(a, pw[0]);
+    qft_slot<R, 0, false>(a, pw[NS - 1]);
+    qft_slot<R, 1, false>(a, pw[NS - 2]);
+    qft_slot<R, 2, false>(a, pw[NS - 3]);
+    if constexpr (NS == 4) qft_slot<R, 3, false>(a, pw[NS - 4]);
   }
 }
 
@@ -834,9 +837,16 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
             }
             bool done = false;
             if constexpr (LR == 4) {
-              if (P.qfull[ph]) {
-                if (P.ops[o0].kind == OP_QFT_FWD) apply_qft_chain4<R, true>(a, pw[0]);
-                else apply_qft_chain4<R, false>(a, pw[0]);
+              const int ns = P.qfull[ph];
+              if (ns) {
+                const bool fwd = P.ops[o0].kind == OP_QFT_FWD;
+                if (ns == 4) {
+                  if (fwd) apply_qft_chain<R, true, 4>(a, pw[0]);
+                  else apply_qft_chain<R, false, 4>(a, pw[0]);
+                } else {
+                  if (fwd) apply_qft_chain<R, true, 3>(a, pw[0]);
+                  else apply_qft_chain<R, false, 3>(a, pw[0]);
+                }
                 done = true;
               }
             }
@@ -1534,17 +1544,18 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
         gmax = std::max(gmax, g);
       }
       if (chain && gmax - gmin == o1 - o0 - 1 && wmax <= 31) P.qchain[p] = (uint8_t)(wmax + 1);
-      // four stages on the four register slots of a 16-amplitude phase,
-      // every slot's stage in the order of the direction
-      if (P.qchain[p] && lr == 4 && o1 - o0 == 4 && wmax >= 3 && qft_full_phases()) {
+      // ns = 3 or 4 stages on register slots 0 .. ns-1 of a 16-amplitude
+      // phase, in the order of the direction
+      const int ns = o1 - o0;
+      if (P.qchain[p] && lr == 4 && (ns == 4 || ns == 3) && wmax >= ns - 1 && qft_full_phases()) {
         const bool fwd = P.ops[o0].kind == OP_QFT_FWD;
         bool full = true;
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < ns; ++i) {
           const TileOp& op = P.ops[o0 + i];
-          full = full && op.kind == P.ops[o0].kind && op.rk == (fwd ? 3 - i : i) &&
-                 op.width == (fwd ? wmax - i : wmax - 3 + i);
+          full = full && op.kind == P.ops[o0].kind && op.rk == (fwd ? ns - 1 - i : i) &&
+                 op.width == (fwd ? wmax - i : wmax - (ns - 1) + i);
         }
-        P.qfull[p] = full ? 1 : 0;
+        P.qfull[p] = full ? (uint8_t)ns : 0;
       }
     }
   } else {
