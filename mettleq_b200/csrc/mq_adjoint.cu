@@ -84,6 +84,59 @@ __device__ __forceinline__ T cmac(T u0, T x0, T u1, T x1) {
   return r;
 }
 
+// complex64 form of the SLOT_MEASURE step on the paired FP32 instructions.
+// With s = (x.y, x.x) the swapped amplitude (formed once per pair and shared
+// by both parts), the products of both components of a pair sit in one
+// paired FMA:
+//   Im conj(l) x = (l (.) s).x - (l (.) s).y,  Re conj(l) x = (l (.) x).x + (l (.) x).y,
+// so gx, gy, gz are paired partial sums folded at the end.  The un-apply
+// u0 x0 + u1 x1 is x0 (.) (u0.x, u0.x) + s0 (.) (-u0.y, u0.y) + x1 (.) (u1.x, u1.x)
+// + s1 (.) (-u1.y, u1.y), chained in the order of cmac, so each lane takes
+// the rounding steps of the scalar form.
+template <int LR, int K>
+__device__ __forceinline__ void adj_slot_c64(float2 (&a)[1 << LR], float2 (&b)[1 << LR], const AdjSlot& S,
+                                             float (&acc)[3]) {
+  auto swp = [](float2 v) { return make_float2(v.y, v.x); };
+  auto neg = [](float2 v) { return make_float2(-v.x, -v.y); };
+  float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax;
+  const bool has_u = S.has_u;
+  float2 U[4][2];  // per matrix entry: (u.x, u.x), (-u.y, u.y)
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const float ux = S.uf[2 * j], uy = S.uf[2 * j + 1];
+    U[j][0] = make_float2(ux, ux);
+    U[j][1] = make_float2(-uy, uy);
+  }
+  auto apply = [&](float2 x0, float2 s0, float2 x1, float2 s1, int row) {
+    const float2* u0 = U[2 * row];
+    const float2* u1 = U[2 * row + 1];
+    return __ffma2_rn(x0, u0[0], __ffma2_rn(s0, u0[1], __ffma2_rn(x1, u1[0], __fmul2_rn(s1, u1[1]))));
+  };
+#pragma unroll
+  for (int r = 0; r < (1 << LR); ++r) {
+    if (r & (1 << K)) continue;
+    const int r1 = r | (1 << K);
+    const float2 x0 = a[r], x1 = a[r1], l0 = b[r], l1 = b[r1];
+    const float2 s0 = swp(x0), s1 = swp(x1);
+    az = __ffma2_rn(l0, s0, az);
+    az = __ffma2_rn(neg(l1), s1, az);
+    ay = __ffma2_rn(l1, x0, ay);
+    ay = __ffma2_rn(neg(l0), x1, ay);
+    ax = __ffma2_rn(l0, s1, ax);
+    ax = __ffma2_rn(l1, s0, ax);
+    if (has_u) {
+      a[r] = apply(x0, s0, x1, s1, 0);
+      a[r1] = apply(x0, s0, x1, s1, 1);
+      const float2 t0 = swp(l0), t1 = swp(l1);
+      b[r] = apply(l0, t0, l1, t1, 0);
+      b[r1] = apply(l0, t0, l1, t1, 1);
+    }
+  }
+  acc[0] += ax.x - ax.y;
+  acc[1] += ay.x + ay.y;
+  acc[2] += az.x - az.y;
+}
+
 // Register bit K: transition values Im <lam|P|psi> for P = X, Y, Z over the
 // thread's pairs (SLOT_MEASURE), then the 2x2 un-apply on both register
 // sets; SLOT_XADD adds c X_q psi to lam instead.
@@ -91,6 +144,12 @@ template <typename R, int LR, int K>
 __device__ __forceinline__ void adj_slot(V2<R> (&a)[1 << LR], V2<R> (&b)[1 << LR], const AdjSlot& S,
                                          R (&acc)[3]) {
   using T = V2<R>;
+  if constexpr (sizeof(R) == 4) {
+    if (S.mode == SLOT_MEASURE) {
+      adj_slot_c64<LR, K>(a, b, S, acc);
+      return;
+    }
+  }
   if (S.mode == SLOT_MEASURE) {
     R gx = 0, gy = 0, gz = 0;
 #pragma unroll
@@ -124,8 +183,8 @@ __device__ __forceinline__ void adj_slot(V2<R> (&a)[1 << LR], V2<R> (&b)[1 << LR
     for (int r = 0; r < (1 << LR); ++r) {
       if (r & (1 << K)) continue;
       const T x0 = a[r], x1 = a[r | (1 << K)];
-      b[r].x += c * x1.x; b[r].y += c * x1.y;
-      b[r | (1 << K)].x += c * x0.x; b[r | (1 << K)].y += c * x0.y;
+      b[r] = caxpy(c, x1, b[r]);
+      b[r | (1 << K)] = caxpy(c, x0, b[r | (1 << K)]);
     }
   }
 }
