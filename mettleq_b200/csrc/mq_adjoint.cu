@@ -556,12 +556,14 @@ static int launch_adj_t(mq_state* psi, mq_state* lam, const AdjParams& P0, doubl
   return MQ_OK;
 }
 
-// Register bits per phase: 3 (more threads per tile and fewer registers per
-// thread than 4, measured faster); complex64 takes 4 with MQ_ADJ_LR=4.
+// Register bits per phase.  complex64: 4 (one phase fewer per sweep; with
+// the paired-FP32 slot a 16-amplitude phase fits 3 CTAs of 128 threads per
+// SM, and the 24-qubit gradient measured 5.55 against 5.66 ms with 3);
+// MQ_ADJ_LR=3 selects 3.  complex128: 3.
 static int adj_lr(int dtype) {
   if (dtype != MQ_C64) return 3;
   const char* v = std::getenv("MQ_ADJ_LR");
-  return (v && std::atoi(v) == 4) ? 4 : 3;
+  return (v && std::atoi(v) == 3) ? 3 : 4;
 }
 
 template <typename R, int LRT>
