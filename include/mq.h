@@ -182,6 +182,16 @@ int mq_adjoint_layer(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubit
  * its gradients back once. */
 int mq_adjoint_layer_async(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits,
                            const double* mats, double* out_dev);
+/* A GF(2) map (rows, c as mq_apply_xor_affine) applied to psi and lam, then
+ * mq_adjoint_layer_async: one backward layer of a circuit whose forward layer
+ * ended with the map's inverse (the CNOT ladder of the layered ansatz; the
+ * reference un-applies it as xor_affine_gather, shaders/xor_affine.py:79-116).
+ * When the map keeps the low tile of the layer's first sweep, that sweep
+ * gathers its input tiles through the map instead of a separate pass over
+ * both states; the results are the same bits either way.  n_q == 0 applies
+ * the map only. */
+int mq_adjoint_layer_xor_async(mq_state* psi, mq_state* lam, const uint64_t* rows, uint64_t c, int n_q,
+                               const int32_t* qubits, const double* mats, double* out_dev);
 
 /* ---- batched circuits (integrations/qiskit.py:505-514 runs them one by one) */
 /* A batch of layered circuits: circuit c has n_qubits[c] qubits (1..30) and

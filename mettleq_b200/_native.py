@@ -67,6 +67,7 @@ SIGNATURES = {
     "mq_apply_pauli_sum": (_I, [_P, _P, _I, _P, _P, _P, _P]),
     "mq_adjoint_layer": (_I, [_P, _P, _I, _P, _P, _P]),
     "mq_adjoint_layer_async": (_I, [_P, _P, _I, _P, _P, _P]),
+    "mq_adjoint_layer_xor_async": (_I, [_P, _P, _P, _U64, _I, _P, _P, _P]),
 }
 
 

@@ -12,8 +12,11 @@ layer from the final state, so no intermediate state is stored:
         for the rotations of every qubit, last to first (exp(-i t G / 2)):
             dE/dt = Im <lam|G|psi>;  psi, lam <- R^dag psi, R^dag lam
 
-The per-layer work is ``mq_adjoint_layer`` (tile sweeps over both states,
-mq_adjoint.cu); ``AdjointEnergy`` exposes it as a ``torch.autograd.Function``.
+The per-layer work is ``mq_adjoint_layer_xor_async`` (tile sweeps over both
+states, mq_adjoint.cu; the ladder's un-apply is gathered by the layer's first
+sweep as it loads its tiles), or ``mq_adjoint_layer`` after a separate
+permutation pass when the gradients are read back per layer;
+``AdjointEnergy`` exposes it as a ``torch.autograd.Function``.
 
 Circuits: ``LayeredAnsatz`` = layers of per-qubit rotation sequences (RX / RY /
 RZ, e.g. the RY+RZ hardware-efficient ansatz) followed by a CNOT ladder
@@ -228,18 +231,25 @@ class AdjointEngine:
         params = np.asarray(params, dtype=np.float64).reshape(A.shape)
         n, L = A.n, A.layers
         inv_rows, inv_c = _ladder_inverse_rows(n)
+        rows = np.ascontiguousarray(np.asarray(inv_rows, dtype=np.uint64))
         qubits = np.arange(n, dtype=np.int32)
         dev = self._grad_buffer(L * 3 * n)
         trans = np.zeros((L, n, 3), dtype=np.float64)
         for i, l in enumerate(reversed(range(L))):
-            if A.ladder:
-                self.psi.apply_xor_affine(inv_rows, inv_c)
-                self.lam.apply_xor_affine(inv_rows, inv_c)
             m = np.ascontiguousarray(_dagger(A.layer_mats(params[l]))).view(np.float64)
             if dev is not None:
-                N.check(self._lib.mq_adjoint_layer_async(self.psi.handle, self.lam.handle, n, _ptr(qubits), _ptr(m),
-                                                         C.c_void_p(dev.data_ptr() + i * 3 * n * 8)))
+                # the ladder's un-apply rides on the layer's first sweep
+                out = C.c_void_p(dev.data_ptr() + i * 3 * n * 8)
+                if A.ladder:
+                    N.check(self._lib.mq_adjoint_layer_xor_async(self.psi.handle, self.lam.handle, _ptr(rows),
+                                                                 int(inv_c), n, _ptr(qubits), _ptr(m), out))
+                else:
+                    N.check(self._lib.mq_adjoint_layer_async(self.psi.handle, self.lam.handle, n, _ptr(qubits),
+                                                             _ptr(m), out))
             else:
+                if A.ladder:
+                    self.psi.apply_xor_affine(inv_rows, inv_c)
+                    self.lam.apply_xor_affine(inv_rows, inv_c)
                 t = np.zeros(3 * n, dtype=np.float64)
                 N.check(self._lib.mq_adjoint_layer(self.psi.handle, self.lam.handle, n, _ptr(qubits), _ptr(m),
                                                    _ptr(t)))

@@ -68,6 +68,17 @@ struct AdjParams {
   uint8_t hi_contig, hi_shift, pad[6];
   BaseRuns runs;  // tile index -> base index (deposit_runs)
   AdjPhase ph[kAdjMaxPhases];
+  // A GF(2) map un-applied on load (TMA form, low tile [0, M)): output
+  // amplitude x of both states is input amplitude perm_c ^ A x, A given by
+  // its columns; A maps the low tile onto itself, so output tile t reads the
+  // input tile of A (t << M) ^ perm_c whole (htab: A of the tile index's
+  // bytes, as EpiDesc).  The outputs go to the states' second buffers
+  // (out[0]: psi, out[1]: lam).
+  uint8_t perm, pad2[3];
+  uint32_t perm_c;
+  uint32_t cols[32];
+  uint32_t htab[768];
+  CUtensorMap out[2];
 };
 
 template <typename R>
@@ -258,6 +269,42 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
     return g;
   };
   auto base_of = [&](uint32_t tile) -> uint32_t { return deposit_runs(tile, P.runs); };
+  // GF(2) map on load: the input tile of output tile t (its base) and the
+  // low offset perm_c ^ A (t << M) leaves inside it; A applied to the thread
+  // part of this thread's chunks (c = tid + k*NT -> amplitude c << CB)
+  auto src_base = [&](uint32_t t, uint32_t& lo) -> uint32_t {
+    lo = 0;
+    if (!P.perm) return base_of(t);
+    const uint32_t b = P.perm_c ^ P.htab[t & 255u] ^ P.htab[256 + ((t >> 8) & 255u)] ^ P.htab[512 + ((t >> 16) & 255u)];
+    lo = b & (uint32_t)(E - 1);
+    return b & ~(uint32_t)(E - 1);
+  };
+  uint32_t perm_at = 0;
+  if (P.perm) {
+#pragma unroll
+    for (int b = 0; b < LT; ++b)
+      if ((tid >> b) & 1) perm_at ^= P.cols[CB + b];
+  }
+  // one state's tile gathered in place: chunk c takes input amplitudes
+  // lo ^ A (c << CB) (complex64: the pair there, swapped when A flips bit 0;
+  // A e_0 = e_0 keeps pairs whole)
+  auto gather = [&](T* buf, uint32_t lo) {
+    float4* c4 = reinterpret_cast<float4*>(buf);
+    float4 v[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+      uint32_t l = lo ^ perm_at;
+#pragma unroll
+      for (int b = 0; b < LCH; ++b)
+        if ((k >> b) & 1) l ^= P.cols[CB + LT + b];
+      const uint32_t ch = l >> CB;
+      const float4 w = c4[ch ^ ((ch >> 3) & 7u)];
+      v[k] = (CB == 1 && (l & 1u)) ? make_float4(w.z, w.w, w.x, w.y) : w;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) c4[slot(k)] = v[k];
+  };
   auto issue = [&](uint32_t tile, int which) {
     const uint32_t gb = base_of(tile) | g_t;
     const uint32_t sp = smem_u32(bufs + which * E), sl = smem_u32(bufs + (2 + which) * E);
@@ -284,7 +331,8 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
   };
   auto tma_issue = [&](uint32_t tile, int which) {
     int32_t c[5];
-    tma_coords(base_of(tile), c);
+    uint32_t lo;
+    tma_coords(src_base(tile, lo), c);
     const uint32_t bar = bar0 + 8u * (uint32_t)which;
     mbar_expect_tx(bar, 2u * P.tma.bytes);
     tma_load_5d(smem_u32(bufs + which * E), &P.tma.src, c, bar);
@@ -315,6 +363,13 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
           bulk_wait_all();
         }
         return;
+      }
+      if (P.perm) {
+        uint32_t lo;
+        (void)src_base(tile, lo);
+        gather(cp, lo);  // each gather reads its buffer, waits, then writes it
+        gather(cl, lo);
+        __syncthreads();
       }
     } else {
       if (next < P.n_tiles) issue(next, cb ^ 1);
@@ -369,8 +424,13 @@ k_adj(V2<R>* psi, V2<R>* lam, const __grid_constant__ AdjParams P, double* __res
       if (tid == 0) {
         int32_t c[5];
         tma_coords(base_of(tile), c);
-        if (P.store_psi) tma_store_5d(&P.tma.src, c, smem_u32(cp));
-        tma_store_5d(&P.tma.dst, c, smem_u32(cl));
+        if (P.perm) {
+          tma_store_5d(&P.out[0], c, smem_u32(cp));
+          tma_store_5d(&P.out[1], c, smem_u32(cl));
+        } else {
+          if (P.store_psi) tma_store_5d(&P.tma.src, c, smem_u32(cp));
+          tma_store_5d(&P.tma.dst, c, smem_u32(cl));
+        }
         bulk_commit();
       }
       continue;
@@ -532,6 +592,13 @@ static int launch_adj_t(mq_state* psi, mq_state* lam, const AdjParams& P0, doubl
     smem += 1024 + 64;  // 1024-byte alignment of the buffers, the mbarriers
     int rc = encode_tile_maps(P.tma, psi->cur_buf(), lam->cur_buf());
     if (rc) return rc;
+    if (P.perm) {  // the outputs: both states' second buffers
+      TmaDesc o = P.tma;
+      rc = encode_tile_maps(o, psi->buf[1 - psi->cur], lam->buf[1 - lam->cur]);
+      if (rc) return rc;
+      P.out[0] = o.src;
+      P.out[1] = o.dst;
+    }
   }
   // one shared-memory size per instance: configure it once
   static std::mutex mu;
@@ -601,7 +668,7 @@ static int dispatch_adj(mq_state* psi, mq_state* lam, const AdjParams& P, double
 // (device memory) on the stream.
 static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarget>& targets,
                          const std::vector<int>& tile_bits, bool store_psi, const std::vector<int>& index,
-                         double* grads_dev) {
+                         double* grads_dev, const uint32_t* perm_cols = nullptr, uint32_t perm_c = 0) {
   const int n = psi->n;
   const int m = (int)tile_bits.size();
   const bool c64 = psi->dtype == MQ_C64;
@@ -620,6 +687,35 @@ static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
   // TMA form for tiles of 10 bits and more (both states move by TMA boxes)
   if (tma_enabled() && m >= 10) {
     if (plan_tma(n, psi->amp_bytes(), tile_bits, P.tma)) P.tma.store = 1;
+  }
+  // a GF(2) map to un-apply first: on load when the sweep is the TMA form of
+  // the low tile [0, m) and the map keeps that tile (complex64: and bit 0),
+  // else as a permutation pass over both states before the sweep
+  if (perm_cols) {
+    bool fuse = store_psi && P.tma.store;
+    for (int k = 0; k < m && fuse; ++k) fuse = tile_bits[k] == k;
+    for (int j = 0; j < m && fuse; ++j) fuse = (perm_cols[j] >> m) == 0;
+    if (fuse && c64) fuse = perm_cols[0] == 1u;
+    if (fuse) {
+      int rc = ensure_alt(psi);
+      if (!rc) rc = ensure_alt(lam);
+      if (rc) return rc;
+      P.perm = 1;
+      P.perm_c = perm_c;
+      for (int j = 0; j < n; ++j) P.cols[j] = perm_cols[j];
+      for (int x = 0; x < 768; ++x) {
+        uint32_t v = 0;
+        for (int bit = 0; bit < 8; ++bit) {
+          const int j = m + 8 * (x >> 8) + bit;
+          if (((x >> bit) & 1) && j < n) v ^= perm_cols[j];
+        }
+        P.htab[x] = v;
+      }
+    } else {
+      int rc = launch_affine_cols(psi, perm_cols, perm_c);
+      if (!rc) rc = launch_affine_cols(lam, perm_cols, perm_c);
+      if (rc) return rc;
+    }
   }
   {
     const int cb = c64 ? 1 : 0;
@@ -669,6 +765,10 @@ static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
   uint32_t grid = 0;
   rc = c64 ? dispatch_adj<float>(psi, lam, P, partials, &grid) : dispatch_adj<double>(psi, lam, P, partials, &grid);
   if (rc) return rc;
+  if (P.perm) {  // both states now live in their second buffers
+    psi->cur ^= 1;
+    lam->cur ^= 1;
+  }
   if (!grads_dev) return MQ_OK;
   AdjCollect C;
   for (int sl = 0; sl < kAdjSlots; ++sl) C.index[sl] = slot_target[sl] < 0 ? -1 : index[slot_target[sl]];
@@ -681,7 +781,7 @@ static int run_adj_sweep(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
 // Tile groups: index bits split as the U(2) layer does, with tiles of at
 // most kAdjTileMax bits (psi and lam share shared memory).
 static int run_adj_layer(mq_state* psi, mq_state* lam, const std::vector<AdjTarget>& all, bool store_psi,
-                         double* grads_dev) {
+                         double* grads_dev, const uint32_t* perm_cols = nullptr, uint32_t perm_c = 0) {
   const int n = psi->n;
   const int tmax = std::min(kAdjTileMax, n);
   const int pas = 4;
@@ -723,15 +823,22 @@ static int run_adj_layer(mq_state* psi, mq_state* lam, const std::vector<AdjTarg
         if (std::find(bits.begin(), bits.end(), b) == bits.end()) bits.push_back(b);
       std::sort(bits.begin(), bits.end());
       if ((int)bits.size() > kAdjTileMax) return fail(MQ_EINVAL, "adjoint tile too large");
-      int rc = run_adj_sweep(psi, lam, part, bits, store_psi, pidx, grads_dev);
+      // a GF(2) map goes with the first sweep (the low group, [0, low))
+      int rc = run_adj_sweep(psi, lam, part, bits, store_psi, pidx, grads_dev, perm_cols, perm_c);
       if (rc) return rc;
+      perm_cols = nullptr;
     }
+  }
+  if (perm_cols) {  // no sweep ran: the map on its own
+    int rc = launch_affine_cols(psi, perm_cols, perm_c);
+    if (!rc) rc = launch_affine_cols(lam, perm_cols, perm_c);
+    if (rc) return rc;
   }
   return MQ_OK;
 }
 
 int adjoint_sweep(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, const double* mats, double* out,
-                  bool out_on_device) {
+                  bool out_on_device, const uint32_t* perm_cols, uint32_t perm_c) {
   const int n = psi->n;
   std::vector<AdjTarget> all;
   std::vector<bool> seen(n, false);
@@ -759,7 +866,7 @@ int adjoint_sweep(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, 
   if (rc) return rc;
   double* dev = grads_on_device ? grads : (grads ? reinterpret_cast<double*>(static_cast<char*>(psi->scratch) + part_bytes) : nullptr);
   if (dev) MQ_CUDA(cudaMemsetAsync(dev, 0, (size_t)3 * n_q * sizeof(double), psi->stream));
-  rc = run_adj_layer(psi, lam, all, true, dev);
+  rc = run_adj_layer(psi, lam, all, true, dev, perm_cols, perm_c);
   if (rc) return rc;
   if (grads && !grads_on_device) {
     MQ_CUDA(cudaMemcpyAsync(grads, dev, (size_t)3 * n_q * sizeof(double), cudaMemcpyDeviceToHost, psi->stream));

@@ -526,6 +526,26 @@ int mq_adjoint_layer_async(mq_state* psi, mq_state* lam, int n_q, const int32_t*
   MQ_TRY_END
 }
 
+int mq_adjoint_layer_xor_async(mq_state* psi, mq_state* lam, const uint64_t* rows, uint64_t c, int n_q,
+                               const int32_t* qubits, const double* mats, double* out_dev) {
+  MQ_TRY_BEGIN
+  int rc = check_pair(psi, lam);
+  if (rc) return rc;
+  if (!rows) return fail(MQ_EINVAL, "null rows");
+  if (n_q < 0) return fail(MQ_EINVAL, "negative qubit count");
+  if (n_q > 0 && (!qubits || !mats || !out_dev)) return fail(MQ_EINVAL, "null layer arrays");
+  uint32_t cols[32];
+  rc = rows_to_cols(psi, rows, c, cols);
+  if (rc) return rc;
+  DeviceGuard g(psi->device);
+  if (n_q == 0) {
+    rc = launch_affine_cols(psi, cols, (uint32_t)c);
+    return rc ? rc : launch_affine_cols(lam, cols, (uint32_t)c);
+  }
+  return adjoint_sweep(psi, lam, n_q, qubits, mats, out_dev, true, cols, (uint32_t)c);
+  MQ_TRY_END
+}
+
 // Allocation-free variant of mq_expval_pauli; see include/mq.h.
 int mq_expval_pauli_static(mq_state* h, int n_words, const uint64_t* xmask, const uint64_t* zmask,
                            const int32_t* ny, double* out) {

@@ -340,8 +340,11 @@ int run_expval_pauli_static(mq_state* h, int n_words, const uint64_t* xmask, con
 
 // Adjoint method (mq_adjoint.cu): one backward layer on (psi, lam), and
 // lam = H psi for H = sum_w zcoef_w Z-word_w + sum_q xcoef_q X_q.
+// perm_cols / perm_c: a GF(2) map out[x] = in[A x ^ c] (A by its columns)
+// un-applied from both states before the layer, fused into the layer's first
+// sweep where that sweep's form allows
 int adjoint_sweep(mq_state* psi, mq_state* lam, int n_q, const int32_t* qubits, const double* mats, double* out,
-                  bool out_on_device);
+                  bool out_on_device, const uint32_t* perm_cols = nullptr, uint32_t perm_c = 0);
 int apply_hamiltonian(mq_state* psi, mq_state* lam, int n_z, const uint64_t* zmasks, const double* zcoef,
                       const double* xcoef, double* energy);
 
