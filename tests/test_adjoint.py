@@ -11,6 +11,7 @@ Tolerances: complex128 adjoint vs parameter shift 1e-9, vs central
 differences 1e-7 (their own O(h^2) error); complex64 adjoint 5e-5.
 """
 import math
+from typing import List, Tuple
 
 import numpy as np
 import pytest
@@ -242,3 +243,89 @@ def test_host_and_device_gradient_readback_agree(monkeypatch):
     finally:
         eng.close()
     assert np.array_equal(g_dev, g_host)
+
+
+def _gf2_map(n: int, m: int, rng, mixing: bool) -> Tuple[List[int], int]:
+    """Rows (qubit k = row k, as mq_apply_xor_affine) and flip of a random
+    invertible map out[x] = in[A x ^ c].  Column operations on the identity:
+    with ``mixing`` False, A maps the low tile [0, m) onto itself and keeps
+    e_0; with ``mixing`` True a high column is added into a low one."""
+    cols = [1 << j for j in range(n)]
+    for _ in range(6 * n):
+        j = int(rng.integers(1, n))
+        i = int(rng.integers(0, n))
+        if i == j or (j < m and i >= m):
+            continue
+        cols[j] ^= cols[i]
+    if mixing:
+        cols[int(rng.integers(1, m))] ^= cols[int(rng.integers(m, n))]
+    rows = [sum(((cols[j] >> (n - 1 - k)) & 1) << j for j in range(n)) for k in range(n)]
+    return rows, int(rng.integers(0, 1 << n))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["complex64", "complex128"])
+@pytest.mark.parametrize("kind", ["low", "mixing", "map_only"])
+def test_adjoint_layer_with_map_equals_separate_pass(dtype, kind):
+    """mq_adjoint_layer_xor_async gives the bits of mq_apply_xor_affine on
+    both states followed by mq_adjoint_layer_async.  That holds for maps that
+    the layer's first sweep gathers on load (they keep its low tile [0, 10)
+    and bit 0), for maps that mix that tile with high bits (a separate pass
+    runs), and for a map with no layer (n_q = 0)."""
+    import ctypes as C
+    import torch
+    from mettleq_b200 import _native as N
+    from mettleq_b200.engine import StateVector
+    n = 16
+    rng = np.random.default_rng({"low": 1, "mixing": 2, "map_only": 3}[kind])
+    rows, c = _gf2_map(n, 10, rng, kind == "mixing")
+    rows_a = np.ascontiguousarray(np.asarray(rows, dtype=np.uint64))
+    n_q = 0 if kind == "map_only" else n
+    qubits = np.arange(n, dtype=np.int32)
+    mats = np.empty((n, 2, 2), dtype=np.complex128)
+    for q in range(n):
+        z = rng.normal(size=(2, 2)) + 1j * rng.normal(size=(2, 2))
+        mats[q] = np.linalg.qr(z)[0]
+    m = np.ascontiguousarray(mats).view(np.float64)
+    p0, l0 = rand_state(n, 11, np.dtype(dtype)), rand_state(n, 12, np.dtype(dtype))
+    lib = N.lib()
+    ptr = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    states = []
+    for _ in range(2):
+        psi = StateVector(n, dtype=dtype)
+        states.append((psi, StateVector(n, dtype=dtype, stream=psi.stream)))  # one stream per pair
+    grads = [torch.zeros(3 * n, dtype=torch.float64, device="cuda") for _ in range(2)]
+    try:
+        for psi, lam in states:
+            psi.set(p0)
+            lam.set(l0)
+        (psi, lam), g = states[0], grads[0]
+        N.check(lib.mq_adjoint_layer_xor_async(psi.handle, lam.handle, ptr(rows_a), c, n_q, ptr(qubits), ptr(m),
+                                               C.c_void_p(g.data_ptr())))
+        (psi2, lam2), g2 = states[1], grads[1]
+        psi2.apply_xor_affine(rows, c)
+        lam2.apply_xor_affine(rows, c)
+        if n_q:
+            N.check(lib.mq_adjoint_layer_async(psi2.handle, lam2.handle, n_q, ptr(qubits), ptr(m),
+                                               C.c_void_p(g2.data_ptr())))
+        out = []
+        for (p, l_), gg in zip(states, grads):
+            p.synchronize()
+            l_.synchronize()
+            out.append((p.get(), l_.get(), gg.cpu().numpy()))
+    finally:
+        for p, l_ in states:
+            l_.close()
+            p.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
+    if kind != "map_only":
+        assert np.any(out[0][2] != 0)
+    # the map itself against the oracle
+    o = OracleSim(n, np.complex128)
+    o.set_state(p0.astype(np.complex128))
+    o.apply_affine(rows, c)
+    if kind == "map_only":
+        tol = 1e-6 if dtype == "complex64" else 1e-15
+        assert np.max(np.abs(out[0][0] - o.state)) < tol
