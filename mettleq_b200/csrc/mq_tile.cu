@@ -1057,10 +1057,17 @@ static int reg_bits(int dtype, int m) {
   const int lr = dtype == MQ_C64 ? env_int("MQ_TILE_LR", 4, 4, 5) : 4;
   return std::min(m, lr);
 }
-static int tile_max(int dtype) {
+// Largest tile of the general sweeps.  complex64 from 29 qubits: 13 bits,
+// where 12-bit tiles (8 targets beside 4 passengers) would need a fourth
+// sweep per layer.  A 30-qubit layer is then 3 sweeps (12 + 9 + 9 targets)
+// and a QFT 3 sweeps.  They moved 25 % less data, held the SM clock at its
+// maximum under the power cap, and measured 3776-3780 against 3620-3630 GB/s
+// with 12-bit tiles.  Smaller states keep 12 (their layers fit 3 sweeps, and
+// more tiles fill the SMs).
+static int tile_max(int dtype, int n) {
   if (dtype != MQ_C64) return 11;
   const int lim = reg_bits(MQ_C64, 13) == 4 ? 13 : 12;
-  return env_int("MQ_TILE_MAX", 12, 6, lim);
+  return env_int("MQ_TILE_MAX", n >= env_int("MQ_TILE13_MIN_QUBITS", 29, 1, 32) ? lim : 12, 6, lim);
 }
 static int passengers() { return env_int("MQ_TILE_PASSENGERS", 4, 0, 5); }
 static bool euler_enabled(const mq_state* h) {
@@ -1073,7 +1080,7 @@ static int min_tile() { return env_int("MQ_TILE_MIN", 10, 1, 12); }
 // one on a batch's states) or the process-wide defaults above.
 static int plan_tile_max(const mq_state* h) {
   if (h->tile_max > 0) return std::min(h->tile_max, h->dtype == MQ_C64 ? 12 : 11);
-  return tile_max(h->dtype);
+  return tile_max(h->dtype, h->n);
 }
 static int plan_passengers(const mq_state* h) { return h->tile_pas >= 0 ? h->tile_pas : passengers(); }
 static int plan_min_tile(const mq_state* h) { return h->tile_min > 0 ? h->tile_min : min_tile(); }
