@@ -53,6 +53,10 @@ constexpr int kMaxPhases = 6;
 // SM overlap one another's loads instead.
 __host__ __device__ constexpr int tile_nbuf(int m, int lt) { return (m >= 13 && lt <= 8) ? 1 : 2; }
 constexpr int kMaxOps = 16;
+// Per register phase, the shared-memory and global offsets of a group's
+// thread bits as two XOR tables each: thread bits 0-3 (16 entries) and 4-8
+// (32 entries); words per phase: 2 x (16 + 32).
+constexpr int kThreadTabWords = 96;
 constexpr int kMaxTileBits = 13;
 
 struct TileOp {
@@ -608,11 +612,14 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
   // shared memory: tile buffers, (TMA) the mbarriers, the launch's phase
   // descriptors, then (MODE >= 2) the permutation columns and the diagonal
   // tables
-  const size_t ph_end = NBUF * sizeof(T) * E + kBarBytes + sizeof(PhaseDesc) * P.n_phases;
+  uint32_t* ttab = reinterpret_cast<uint32_t*>(smem + NBUF * sizeof(T) * E + kBarBytes + sizeof(PhaseDesc) * P.n_phases);
+  const size_t ph_end = NBUF * sizeof(T) * E + kBarBytes + sizeof(PhaseDesc) * P.n_phases +
+                        sizeof(uint32_t) * kThreadTabWords * P.n_phases;
   uint32_t* ecols = reinterpret_cast<uint32_t*>(smem + ph_end);
   T* qreg = reinterpret_cast<T*>(smem + ph_end);  // MODE 1: per op, the register factors treg[32]
   T* elut = reinterpret_cast<T*>(smem + ph_end + 128);
   const int tid = threadIdx.x;
+  const uint32_t t_lo = (uint32_t)tid & 15u, t_hi = (uint32_t)tid >> 4;
   if constexpr (TMA) {
     if (tid == 0) {
       for (int b = 0; b < NBUF; ++b) mbar_init(bar0 + 8u * b, 1);
@@ -624,6 +631,23 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
     const uint32_t* srcw = reinterpret_cast<const uint32_t*>(&P.ph[0]);
     uint32_t* dstw = reinterpret_cast<uint32_t*>(phs);
     for (uint32_t w = tid; w < words; w += NT) dstw[w] = srcw[w];
+  }
+  // the thread tables of every phase: a group's offsets over the thread's
+  // bits of its index q (q's bits below LT are the thread id's) are then two
+  // table reads, the same for every tile of the sweep
+  constexpr int TLO = LT < 4 ? LT : 4;
+  static_assert(LT - TLO <= 5, "thread tables hold 5 high thread bits");
+  for (int w = tid; w < P.n_phases * kThreadTabWords; w += NT) {
+    const int p = w / kThreadTabWords, r = w % kThreadTabWords;
+    const uint32_t* grp = (r >= 48) ? P.ph[p].g_grp : P.ph[p].s_grp;
+    const int e = r % 48;
+    const bool hi = e >= 16;
+    const uint32_t bits = hi ? (uint32_t)(e - 16) : (uint32_t)e;
+    const int j0 = hi ? TLO : 0, nb = hi ? LT - TLO : TLO;
+    uint32_t v = 0;
+    for (int j = 0; j < nb; ++j)
+      if ((bits >> j) & 1u) v ^= grp[j0 + j];
+    ttab[w] = v;
   }
   if constexpr (!QFT) {
     if (P.mats_dev) {
@@ -794,13 +818,17 @@ k_tile(const V2<R>* src, V2<R>* dst, const __grid_constant__ PT P) {
 #pragma unroll
       for (int g = 0; g < GPT; ++g) {
         const uint32_t q = (uint32_t)tid + (uint32_t)g * NT;
-        uint32_t sq = 0, gq = base;
+        // thread bits from the phase's tables, the bits of g (above LT) from
+        // the descriptor (compile-time selected)
+        const uint32_t* tt = ttab + ph * kThreadTabWords;
+        uint32_t sq = tt[t_lo] ^ tt[16 + t_hi], gq = base;
 #pragma unroll
-        for (int j = 0; j < M - LR; ++j)
+        for (int j = LT; j < M - LR; ++j)
           if ((q >> j) & 1) sq ^= D.s_grp[j];
         if (need_g) {
+          gq |= tt[48 + t_lo] | tt[64 + t_hi];
 #pragma unroll
-          for (int j = 0; j < M - LR; ++j)
+          for (int j = LT; j < M - LR; ++j)
             if ((q >> j) & 1) gq |= D.g_grp[j];
         }
         // complex64 with tile bit 0 in register slot 0: amplitudes r, r+1 share
@@ -1598,7 +1626,7 @@ static int run_sweep(mq_state* h, Sweep& sw, const std::vector<int>& op_phase, c
   P.need_tw = (qft && sw.need_tw && h->dtype == MQ_C64) ? 1 : 0;
   P.has_scale = sw.has_scale ? 1 : 0;
   P.scale = sw.has_scale ? sw.scale : 1.0;
-  size_t smem = 2 * (h->amp_bytes() << m) + sizeof(PhaseDesc) * sw.phases.size();
+  size_t smem = 2 * (h->amp_bytes() << m) + (sizeof(PhaseDesc) + sizeof(uint32_t) * kThreadTabWords) * sw.phases.size();
   if (P.need_tw) {
     int rc = ensure_qft_twiddles(h);
     if (rc) return rc;
