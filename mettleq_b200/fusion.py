@@ -521,9 +521,10 @@ def _split_bits(n: int, tmax: int, pas: int) -> List[Tuple[int, int]]:
 
 def expected_sweeps(layer: dict, n: int, dtype: str = "complex64") -> int:
     """Full-state passes a fused layer launches (for execution reports), from
-    the engine's default tile plan (12-bit complex64 / 11-bit complex128
-    tiles, 4 low passenger bits)."""
-    tmax = 12 if dtype == "complex64" else 11
+    the engine's default tile plan: complex64 tiles of 13 bits from 29 qubits
+    and of 12 bits below (mq_tile.cu tile_max), complex128 tiles of 11 bits,
+    4 low passenger bits."""
+    tmax = (13 if n >= 29 else 12) if dtype == "complex64" else 11
     pas = 4
     name = layer["name"]
     groups = _split_bits(n, tmax, pas)

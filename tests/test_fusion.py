@@ -76,10 +76,13 @@ def test_pair_terms_fuse_into_one_layer_per_family_run():
     assert len(pairs[0]["bonds"]) == n and len(pairs[1]["bonds"]) == n
     vec = rand_state(n, 4, np.complex128)
     assert np.max(np.abs(interpret(layers, n, vec) - reference(ops, n, vec))) < 1e-12
-    # at 30 qubits a chain over every qubit is two U(2) layers: 2 x 4 sweeps
+    # at 30 qubits a chain over every qubit is two U(2) layers: 2 x 3 sweeps
+    # (13-bit tiles: index bits 0-11, 12-20, 21-29; 12-bit tiles would need 4)
     chain = {"name": "_PAIRLAYER", "kind": "XX", "bonds": [(i, i + 1) for i in range(29)], "thetas": [0.1] * 29}
-    assert F.expected_sweeps(chain, 30) == 8
+    assert F.expected_sweeps(chain, 30) == 6
     assert F.expected_sweeps(pairs[0], 30) == 2  # wires 0..6: the top bit group only
+    chain28 = {"name": "_PAIRLAYER", "kind": "XX", "bonds": [(i, i + 1) for i in range(27)], "thetas": [0.1] * 27}
+    assert F.expected_sweeps(chain28, 28) == 6  # 12-bit tiles: bits 0-11, 12-19, 20-27
 
 
 def reference(ops, n, vec):
@@ -275,5 +278,6 @@ def test_expected_sweeps_of_fused_config_layer():
     ops, _ = c.ops()
     layers = F.fuse(ops, 30)
     assert [L["name"] for L in layers] == ["_LAYER"]
-    # 30 index bits in four tile groups; diagonal and ladder ride on the low sweep
-    assert F.expected_sweeps(layers[0], 30) == 4
+    # 30 index bits in three tile groups (13-bit tiles); diagonal and ladder
+    # ride on the low sweep
+    assert F.expected_sweeps(layers[0], 30) == 3
