@@ -7,17 +7,18 @@
 // sector per 8 useful bytes.
 //
 // Here the permutation is done by tiles that are coalesced on BOTH sides.
-// With P low passenger bits (16 amplitudes = 128 B):
+// With P low passenger bits (32 amplitudes = 256 B by default):
 //   S_in  = span(e_0..e_{P-1}, A e_0..A e_{P-1}), padded with unit vectors to
 //           dimension D (1024 amplitudes per tile);
 //   S_out = A^{-1} S_in, which contains e_0..e_{P-1} by construction.
 // Each output coset y in h ^ S_out reads from the input coset A h ^ c ^ S_in:
-// both cosets are unions of 128-byte runs.  A CTA loads the input coset in
+// both cosets are unions of 2^P-amplitude runs.  A CTA loads the input coset in
 // address order into shared memory and writes the output coset in address
 // order, mapping slots through the D x D coordinate matrix of A on the tile.
 // Any invertible A (CNOT/X/SWAP runs, SWAP-network wire permutations, random
 // GF(2) layers) costs exactly one read and one write of the state.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -232,7 +233,13 @@ int launch_affine_cols(mq_state* h, const uint32_t* cols, uint32_t c) {
   int rc = ensure_alt(h);
   if (rc) return rc;
   const int D = std::min(10, n);
-  const int pas = std::min(4, D / 2);
+  // passenger bits: both cosets are unions of 2^pas-amplitude runs (5: 256
+  // bytes, all of D = 10 then spanned by e_j and A e_j, j < 5; the random
+  // 30-qubit GF(2) layer measured 3.13 ms against 3.57-3.60 ms with 4, 128
+  // bytes); MQ_PERM_PASSENGERS overrides
+  const char* pv = std::getenv("MQ_PERM_PASSENGERS");
+  const int pas_want = (pv && *pv) ? std::max(1, std::min(5, std::atoi(pv))) : 5;
+  const int pas = std::min(pas_want, D / 2);
   // input-side tile basis
   Echelon ein;
   std::vector<uint32_t> vin;
