@@ -9,6 +9,8 @@
 * Plain statevector at scale, 30 qubits: too large for the oracle, so a
   size-independent property checks it: the complex64 state against the same
   circuit run in complex128 on the GPU (infidelity <= 1e-9) and its norm.
+  At 31 qubits (the largest register) the 13-bit and 12-bit tile plans
+  against each other the same way.
 * Its random GF(2) layer at 28 qubits, bit-exact against the oracle's source
   map evaluated on the GPU; its fused config layer at 28 qubits against the
   same layer as separate passes on other kernels; its QFT at 28 qubits on
@@ -62,9 +64,10 @@ def test_plain_config_20_qubits_against_the_oracle():
     dev.close()
 
 
-def _device_infidelity(sv64, sv128):
-    """(1 - |<a|b>|^2 / (<a|a><b|b>), <a|a>) of two device states, summed on the GPU
-    in complex128 (the 30-qubit states stay in device memory)."""
+def _device_infidelity(sv64, sv128, b_typestr="<c16"):
+    """(1 - |<a|b>|^2 / (<a|a><b|b>), <a|a>) of two device states (a complex64,
+    b of b_typestr), summed on the GPU in complex128 (the 30-qubit states stay
+    in device memory)."""
     import torch
 
     class _Dev:
@@ -76,18 +79,47 @@ def _device_infidelity(sv64, sv128):
     sv64.synchronize()
     sv128.synchronize()
     a = torch.as_tensor(_Dev(sv64.device_ptr(), n, "<c8"), device="cuda:0")
-    b = torch.as_tensor(_Dev(sv128.device_ptr(), n, "<c16"), device="cuda:0")
+    b = torch.as_tensor(_Dev(sv128.device_ptr(), n, b_typestr), device="cuda:0")
     ov = torch.zeros((), dtype=torch.complex128, device="cuda:0")
     na = torch.zeros((), dtype=torch.float64, device="cuda:0")
     nb = torch.zeros((), dtype=torch.float64, device="cuda:0")
     for s in range(0, n, 1 << 26):
         x = a[s:s + (1 << 26)].to(torch.complex128)
-        y = b[s:s + (1 << 26)]
+        y = b[s:s + (1 << 26)].to(torch.complex128)
         ov += torch.vdot(x, y)
         na += torch.vdot(x, x).real
         nb += torch.vdot(y, y).real
     torch.cuda.synchronize()
     return 1.0 - (ov.abs() ** 2 / (na * nb)).item(), na.item()
+
+
+def test_31_qubits_tile_plans_agree(monkeypatch):
+    """The largest register: at 31 qubits the 13-bit tile plan runs a fused
+    layer as three sweeps whose low sweep is a 13-bit tile of 13 targets, and
+    a QFT as three sweeps; the 12-bit plan (MQ_TILE_MAX=12) runs four.  Both
+    give the same state of 3 config layers, a QFT and a GF(2) layer to within
+    complex64 rounding (infidelity on the GPU in complex128, norm 1)."""
+    from mettleq_b200 import workloads as W
+    from mettleq_b200.engine import StateVector
+    n = 31
+    circ = W.scale_circuit(n, 3, seed=0, qft_every=3)
+    monkeypatch.delenv("MQ_TILE_MAX", raising=False)
+    sv13 = StateVector(n, "complex64")
+    W.run_circuit_layers(sv13, circ)
+    sweeps13 = sv13.counters()[1]
+    monkeypatch.setenv("MQ_TILE_MAX", "12")
+    sv12 = StateVector(n, "complex64")
+    W.run_circuit_layers(sv12, circ)
+    sweeps12 = sv12.counters()[1]
+    monkeypatch.delenv("MQ_TILE_MAX", raising=False)
+    try:
+        infid, norm = _device_infidelity(sv13, sv12, "<c8")
+    finally:
+        sv12.close()
+        sv13.close()
+    assert sweeps13 < sweeps12
+    assert abs(1.0 - norm) <= 1e-5
+    assert infid <= 1e-9
 
 
 def test_scale_config_30_qubits_against_complex128():
